@@ -1,0 +1,426 @@
+#!/usr/bin/env python
+"""bench.py -- DFS nodes/s and wall ms of the B200 N-Queens counting path.
+
+One step counts a whole board on one GPU: every half-board prefix of `k` rows
+(the reference's task list, src/n_queens.cpp:74-113) goes through the
+persistent DFS kernel, and the step's count is checked bit-exact against the
+reference's published total (README.md / logs).  The default workload is
+N=21, k=6 (4,470,757 prefix tasks).
+
+Reported (one JSON line from rank 0):
+  value      DFS nodes/s with the tasks resident in HBM (kernel + queue reset,
+             CUDA events on the launching stream, L2 flushed between steps);
+  e2e        the same metric through the public C ABI call nq_count (host
+             expansion, pinned H2D copy of the tasks, kernel, D2H of the
+             result), host wall clock per step;
+  roofline   integer-issue roofline: 22 warp-issue slots per DFS node against
+             numSMs x 4 schedulers x clock;
+  cpu_baseline  the reference's own CPU recursion (oracle/_ref, all host
+             threads) on a seeded sample of the same tasks.
+
+`--impl reference` times only that reference CPU path (rank 0; other ranks
+exit 0).  Under torchrun each rank counts the same board on its own GPU
+(replicas: the reference's multi-GPU split is out of scope), and the time is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+I_ALG = 22  # algorithmic warp-issue slots per DFS node (fixed cost model)
+METRIC = "DFS nodes/s (exact whole-board count, 1 B200)"
+
+# Whole-board workloads: published totals (README.md:16-25, logs/5090.log) and
+# DFS node totals (placements into rows k..N-2, counted by the kernel's node
+# statistics and, up to N=17, by the CPU oracle).
+WORKLOADS = {
+    "n16k5": dict(N=16, k=5, total=14772512, nodes=563126914),
+    "n19k6": dict(N=19, k=6, total=4968057848, nodes=228483606026),
+    "n20k6": dict(N=20, k=6, total=39029188884, nodes=1865470950135),
+    "n21k6": dict(N=21, k=6, total=314666222712, nodes=None),
+    "n22k6": dict(N=22, k=6, total=2691008701644, nodes=None),
+}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="n21k6")
+    ap.add_argument("--cpu-seconds", type=float, default=8.0, help="CPU work per reference-sample step")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while running (clocks and throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+            if self.gpu_id:
+                cmd += ["-i", self.gpu_id]
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+                except ValueError:
+                    continue
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        reasons = sorted({n for _, _, flags in rows for n, f in zip(self.NAMES, flags) if f.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- CPU reference sample
+def reference_sample(N: int, k: int, seconds: float, seed: int = 12345):
+    """A seeded random sample of the workload's prefix tasks sized for about
+    `seconds` of the reference's CPU recursion on all host threads; returns
+    (aos int32[n,3], nodes, counts, threads, kind)."""
+    import oracle
+    from n_queens_b200 import workloads  # noqa: F401  (keeps the import surface uniform)
+
+    cols, ld, rd = oracle.expand(N, k)
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(cols.size)
+    threads = os.cpu_count() or 1
+    kind = "reference" if oracle.ref_available() else "port"
+
+    def run(idx):
+        aos = np.stack([cols[idx], ld[idx], rd[idx]], axis=1).view(np.int32)
+        t = time.perf_counter()
+        if kind == "reference":
+            oracle.ref_count_tasks(N, aos, threads=threads)
+        else:
+            oracle.count_tasks(N, cols[idx], ld[idx], rd[idx], threads=threads)
+        return time.perf_counter() - t
+
+    n = 4 * threads
+    while True:
+        dt = run(perm[:n])
+        if dt > 0.5 or n >= cols.size:
+            break
+        n = min(cols.size, n * 4)
+    n = int(min(cols.size, max(n, n * seconds / max(dt, 1e-3))))
+    idx = np.sort(perm[:n])
+    cnt, nodes = oracle.count_tasks(N, cols[idx], ld[idx], rd[idx], nodes=True, threads=threads)
+    aos = np.stack([cols[idx], ld[idx], rd[idx]], axis=1).view(np.int32)
+    return aos, int(nodes.sum()), cnt, threads, kind
+
+
+def time_reference(N, aos, threads, kind, cnt):
+    import oracle
+
+    t = time.perf_counter()
+    if kind == "reference":
+        s2, per = oracle.ref_count_tasks(N, aos, threads=threads, per_task=True)
+        ok = np.array_equal(per.view(np.uint64), cnt)
+    else:
+        c = aos.view(np.uint32)
+        per = oracle.count_tasks(N, c[:, 0], c[:, 1], c[:, 2], threads=threads)
+        ok = np.array_equal(per, cnt)
+    dt = time.perf_counter() - t
+    if not ok:
+        raise SystemExit("reference sample: per-task counts disagree with the oracle")
+    return dt
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ----------------------------------------------------------------------------- distributed
+def dist_init(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl" if n_gpus > 0 else "gloo", timeout=datetime.timedelta(seconds=900))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(world, x: float) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def traffic_from_profile(name: str):
+    """DRAM bytes per launch of the DFS kernel, from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ----------------------------------------------------------------------------- arms
+def run_reference(args, world, rank):
+    wl = WORKLOADS[args.workload]
+    if rank != 0:
+        return
+    N, k = wl["N"], wl["k"]
+    aos, nodes, cnt, threads, kind = reference_sample(N, k, args.cpu_seconds)
+    for _ in range(args.warmup):
+        time_reference(N, aos, threads, kind, cnt)
+    times = [time_reference(N, aos, threads, kind, cnt) for _ in range(args.steps)]
+    total = sum(times)
+    value = nodes * args.steps / total
+    sample = (f"{aos.shape[0]} of {oracle_tasks(N, k)} N={N} k={k} prefix tasks (seeded uniform sample, "
+              f"{nodes} DFS nodes), reference n_queens() recursion, {threads} threads on {cpu_model()}")
+    line = {
+        "metric": METRIC, "value": value, "unit": "nodes/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 masks / u64 counts",
+        "data": "synthetic (the reference's own prefix tasks; deterministic)",
+        "config": {"workload": f"N={N} k={k} whole-board count", "N": N, "k": k, "tasks_per_step": int(aos.shape[0])},
+        "cpu_baseline": {"value": value, "unit": "nodes/s", "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "nodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def oracle_tasks(N, k):
+    import oracle
+
+    return int(oracle.lib.nq_oracle_expand(N, k, None, None, None, 0))
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import n_queens_b200 as nq
+
+    wl = WORKLOADS[args.workload]
+    N, k, want = wl["N"], wl["k"], wl["total"]
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    props = torch.cuda.get_device_properties(dev)
+    sms = props.multi_processor_count
+    gpu_uuid = None
+    try:
+        gpu_uuid = "GPU-" + str(props.uuid)
+    except Exception:
+        pass
+
+    # Tasks resident in HBM for the device-timed loop.
+    cols, ld, rd = nq.expand(N, k)
+    ntasks = cols.size
+    tc = torch.from_numpy(cols.view(np.int32)).to(dev)
+    tl = torch.from_numpy(ld.view(np.int32)).to(dev)
+    tr = torch.from_numpy(rd.view(np.int32)).to(dev)
+    levels = N - 1 - k
+    cfg = nq.Config()
+    cfg.device = local
+    cfg.stack_levels = levels
+    stream = torch.cuda.current_stream(dev)
+    nslots = max(args.steps, args.warmup, 1)
+    sums = torch.zeros((nslots, 2), dtype=torch.int64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    nodes = wl["nodes"]
+    if nodes is None:
+        r = nq.count(N, k, config=cfg, nodes=True)
+        assert r.total == want, (r.total, want)
+        nodes = r.nodes
+
+    def check(nsteps):
+        s = sums[:nsteps].cpu().numpy()
+        for i in range(nsteps):
+            if 2 * int(s[i, 0]) != want or int(s[i, 1]) != 0:
+                raise SystemExit(f"step {i}: count {2 * int(s[i, 0])} status {int(s[i, 1])}, want {want}")
+
+    def step(i):
+        sp = sums[i]
+        rc = nq.lib.nq_count_tasks_device(N, tc.data_ptr(), tl.data_ptr(), tr.data_ptr(), ntasks, None, None,
+                                          sp.data_ptr(), nq.ctypes.byref(cfg), stream.cuda_stream)
+        if rc != 0:
+            raise SystemExit(f"nq_count_tasks_device: {nq.status_string(rc)} {nq.last_error()}")
+
+    for i in range(args.warmup):
+        flush.zero_()
+        step(i)
+    torch.cuda.synchronize()
+    check(args.warmup)
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(gpu_uuid) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            starts[i].record(stream)
+            step(i)
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    clocks = clk.summary()
+    check(args.steps)
+    kern_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    t_local = sum(kern_ms) / 1000.0
+    t_max = max_over_ranks(world, t_local)
+    value = world * nodes * args.steps / t_max
+
+    # End to end through the public C ABI (nq_count): expansion, pinned H2D,
+    # kernel, D2H of the result words.
+    e2e = None
+    if not args.no_e2e:
+        ecfg = nq.Config()
+        ecfg.device = local
+        r = nq.count(N, k, config=ecfg)  # sizes the library's buffers for this board
+        assert r.total == want
+        barrier(world)
+        walls, stats = [], []
+        for i in range(args.steps):
+            t0 = time.perf_counter()
+            r = nq.count(N, k, config=ecfg)
+            walls.append(time.perf_counter() - t0)
+            if r.total != want:
+                raise SystemExit(f"e2e step {i}: count {r.total}, want {want}")
+            stats.append(r.stats)
+        barrier(world)
+        e_max = max_over_ranks(world, sum(walls))
+        e2e = {
+            "value": world * nodes * args.steps / e_max, "unit": "nodes/s",
+            "wall_ms_per_step": 1000 * e_max / args.steps,
+            "h2d_bytes_per_step": 12 * ntasks, "d2h_bytes_per_step": 24,
+            "breakdown_ms": {key: statistics.mean(s[key] for s in stats)
+                             for key in ("expand_ms", "h2d_ms", "kernel_ms", "d2h_ms", "total_ms")},
+        }
+
+    peak_clock = None
+    try:
+        peak_clock = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("sm_max_mhz")
+    except (OSError, ValueError):
+        pass
+    peak_src = "MEASURED_PEAKS.json sm_max_mhz"
+    if not peak_clock:
+        peak_clock, peak_src = clocks.get("sm_max_mhz") or 1965.0, "sampled clocks.max.sm"
+    achieved = (nodes * args.steps / t_local) * I_ALG / 32 / 1e9
+    peak = sms * 4 * peak_clock * 1e6 / 1e9
+    roof = {
+        "bound": "int-issue", "achieved": achieved, "peak": peak, "unit": "Gwarp-inst/s", "frac": achieved / peak,
+        "traffic": traffic_from_profile(f"dfs_kernel_n{N}k{k}.md"),
+        "note": (f"achieved = DFS nodes/s x {I_ALG} issue slots / 32 lanes; peak = {sms} SMs x 4 schedulers x "
+                 f"{peak_clock:.0f} MHz ({peak_src}); traffic = ncu DRAM bytes per launch"),
+    }
+    if clocks.get("sm_mhz"):
+        roof["frac_at_sampled_clock"] = achieved / (sms * 4 * clocks["sm_mhz"] * 1e6 / 1e9)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        aos, snodes, cnt, threads, kind = reference_sample(N, k, args.cpu_seconds)
+        dt = time_reference(N, aos, threads, kind, cnt)
+        cpu = {"value": snodes / dt, "unit": "nodes/s", "cores": threads, "kind": kind,
+               "sample": (f"{aos.shape[0]} of {ntasks} N={N} k={k} prefix tasks (seeded uniform sample, "
+                          f"{snodes} DFS nodes) through the reference n_queens() recursion, {threads} threads "
+                          f"on {cpu_model()}")}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "nodes/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 masks / u64 counts",
+            "data": "synthetic (the reference's own prefix tasks; deterministic)",
+            "config": {"workload": f"N={N} k={k} whole-board count", "N": N, "k": k, "tasks": int(ntasks),
+                       "dfs_nodes": int(nodes), "count": int(want), "schedule": "plain dynamic fetch",
+                       "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"replicas x{world}",
+                       "stack_levels": levels},
+            "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+            "gpu_launches": args.steps,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_init(args.gpus if args.impl == "ours" else 0)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

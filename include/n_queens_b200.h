@@ -1,0 +1,153 @@
+/*
+ * n_queens_b200.h -- C ABI of the B200 (sm_100a) N-Queens solution counter.
+ *
+ * This is the drop-in boundary for the counting path of ygch/n_queens:
+ *
+ *   host prefix expander  ->  device task queue  ->  persistent DFS kernel
+ *   (src/n_queens.cpp:74-113)  (src/n_queens_cuda.cu:8)  (src/n_queens_cuda.cu:9-82)
+ *   -> uint64 reduction (src/n_queens_cuda.cu:181-183)
+ *
+ * Plain pointers and sizes only.  The caller owns every host buffer; the
+ * library owns its device buffers (kept per device and reused between calls)
+ * except in the *_device entry, where the caller passes device pointers.
+ * Every entry returns an nq_status; nothing here calls exit() (the reference's
+ * CU_SAFE_CALL in src/macro.h:40-49 does).  Calls on one device must come from
+ * one host thread at a time; a per-device mutex serialises them.
+ *
+ * Semantics of one task (cols, ld, rd, N): exactly the reference recursion
+ * n_queens(N, cur, left, right) of src/n_queens.cpp:8-21 -- a task whose
+ * column mask equals (1<<N)-1 counts 1; otherwise every free column
+ * last & ~(cur|left|right) is tried, left shifts left (bits past 31 drop) and
+ * right shifts right arithmetically, as the reference's `int` arithmetic does.
+ */
+#ifndef N_QUEENS_B200_H
+#define N_QUEENS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NQ_ABI_VERSION 1
+
+/* Largest board.  The reference CLI stops at 28 (src/main.cpp:10); the
+ * library takes any N < 32, since masks are 32-bit. */
+#define NQ_MAX_N 31
+
+typedef enum nq_status {
+    NQ_OK = 0,
+    NQ_ERR_ARG = -1,       /* an argument is out of range or a pointer is NULL */
+    NQ_ERR_NO_DEVICE = -2, /* no CUDA device (cuda_n_queens then returns -1, src/n_queens_cuda.cu:105-108) */
+    NQ_ERR_CUDA = -3,      /* a CUDA runtime call failed; see nq_last_error() */
+    NQ_ERR_OOM = -4,       /* device or pinned-host allocation failed */
+    NQ_ERR_DEPTH = -5,     /* a task needs more stack levels than the launch provides */
+    NQ_ERR_TIMEOUT = -6,   /* the kernel reached cfg->time_limit_ms and stopped; the counts are partial */
+    NQ_ERR_NO_KERNEL = -7  /* the library has no sm_100a image for this device */
+} nq_status;
+
+/* Task order.  NQ_ORDER_PLAIN hands tasks out in expander order through one
+ * atomic ticket (the reference's dynamic fetch, src/n_queens_cuda.cu:10,80);
+ * NQ_ORDER_GIVEN uses the caller's permutation (nq_config.order), e.g. a
+ * longest-first schedule from the learned cost model. */
+enum { NQ_ORDER_PLAIN = 0, NQ_ORDER_GIVEN = 1 };
+
+/* Launch parameters; zero-initialise and set what you need.  Zero means
+ * "default" (the autotuned or built-in choice) for every field. */
+typedef struct nq_config {
+    int block_threads;      /* threads per CTA: 64..1024, multiple of 32 */
+    int blocks_per_sm;      /* resident CTAs per SM for the persistent grid */
+    int stack_levels;       /* per-lane DFS stack slots (>= N-1-rows)  */
+    int steal;              /* 0 = default (on), 1 = on, -1 = off: in-warp work donation */
+    int inner_steps;        /* DFS steps between warp refill checks (multiple of 4) */
+    int order_kind;         /* NQ_ORDER_PLAIN or NQ_ORDER_GIVEN */
+    const uint32_t *order;  /* NQ_ORDER_GIVEN: queue position -> task index (host or device
+                               pointer, matching the entry's other task arrays) */
+    uint32_t time_limit_ms; /* 0 = none; else the kernel stops after this long (NQ_ERR_TIMEOUT) */
+    int device;             /* CUDA device ordinal (default 0) */
+    int reserved[6];
+} nq_config;
+
+/* Timings and sizes of one call (all optional outputs). */
+typedef struct nq_stats {
+    double expand_ms;   /* host prefix expansion */
+    double h2d_ms;      /* task upload (event-timed) */
+    double kernel_ms;   /* queue reset + DFS kernel + reduction (event-timed) */
+    double d2h_ms;      /* result download (event-timed) */
+    double total_ms;    /* wall time of the whole call */
+    int64_t tasks;      /* number of tasks */
+    uint64_t nodes;     /* DFS nodes, when the entry was asked to count them */
+    int grid;           /* CTAs launched */
+    int block_threads;  /* threads per CTA */
+    int stack_levels;   /* stack slots per lane */
+    int smem_bytes;     /* dynamic shared memory per CTA */
+    int reserved[5];
+} nq_stats;
+
+/* One independent completion-counting problem of the batched entry. */
+typedef struct nq_instance {
+    int32_t N;     /* board size, 1..NQ_MAX_N */
+    uint32_t cols; /* columns taken by the pre-placed rows */
+    uint32_t ld;   /* left-diagonal attacks on the next row */
+    uint32_t rd;   /* right-diagonal attacks on the next row */
+} nq_instance;
+
+/* Library and error reporting. */
+int nq_abi_version(void);
+const char *nq_status_string(int status);
+/* Text of the last CUDA error seen by this thread (empty if none). */
+const char *nq_last_error(void);
+/* Number of CUDA devices (0 when none); returns NQ_OK or NQ_ERR_CUDA. */
+int nq_device_count(int *count);
+
+/* Host prefix expander.  Replaces partial_n_queens + partial_n_queens_for_odd
+ * (src/n_queens.cpp:74-113) as cuda_n_queens calls them
+ * (src/n_queens_cuda.cu:91-95): every non-attacking placement of rows
+ * 0..rows-1 with row 0 in columns [0, N/2), then for odd N the middle-column
+ * pass, in the reference's order, as SoA uint32 triples.  Writes at most cap
+ * tasks and stores the full count in *n_tasks (call with cap = 0 to size).
+ * threads <= 0 uses every host core. */
+int nq_expand(int N, int rows, uint32_t *cols, uint32_t *ld, uint32_t *rd, int64_t cap, int64_t *n_tasks,
+              int threads);
+
+/* Whole-board count.  Replaces cuda_n_queens (src/n_queens_cuda.cu:84-186)
+ * on one device: expand, upload, count, and return 2 x the sum of the
+ * per-prefix counts in *total (the reference's x2 mirror reduction,
+ * src/n_queens_cuda.cu:181-183).  Requires 2 <= N <= NQ_MAX_N and
+ * 1 <= rows <= N-2 (src/main.cpp:21-24).  If nodes is not NULL the DFS
+ * node total of the same decomposition is counted as well (slower). */
+int nq_count(int N, int rows, const nq_config *cfg, uint64_t *total, uint64_t *nodes, nq_stats *stats);
+
+/* Counts over a caller-built task list in host memory.  Replaces the
+ * per-GPU upload / launch / download of src/n_queens_cuda.cu:156-177 with
+ * the per-task semantics of n_queens() (src/n_queens.cpp:8-21).
+ * per_task[i] (optional) receives task i's completions, nodes_per_task[i]
+ * (optional) its DFS nodes; *sum receives the plain sum of the counts
+ * (no x2).  n may be 0. */
+int nq_count_tasks(int N, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd, int64_t n,
+                   uint64_t *per_task, uint64_t *nodes_per_task, uint64_t *sum, const nq_config *cfg,
+                   nq_stats *stats);
+
+/* The same over device-resident tasks (device pointers, already in HBM),
+ * enqueued on `stream` (a cudaStream_t; NULL = legacy default stream).
+ * d_per_task / d_nodes are optional device arrays of n uint64 (overwritten);
+ * d_sum is a device uint64 (overwritten).  Returns after enqueueing; the
+ * caller synchronises the stream.  Uses the library's device scratch for the
+ * queue and the per-CTA partials, so calls on one device must not overlap. */
+int nq_count_tasks_device(int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd, int64_t n,
+                          uint64_t *d_per_task, uint64_t *d_nodes, uint64_t *d_sum, const nq_config *cfg,
+                          void *stream);
+
+/* Batched independent instances of uneven N and partial boards in one
+ * persistent launch.  Each instance is split into subtasks at split_rows
+ * extra rows (0 = autotuned) and out[i] receives its completions (no
+ * symmetry factor, as n_queens() counts them). */
+int nq_count_batch(const nq_instance *inst, int64_t n, int split_rows, uint64_t *out, const nq_config *cfg,
+                   nq_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* N_QUEENS_B200_H */

@@ -1,0 +1,624 @@
+// capi.cu -- the C ABI (include/n_queens_b200.h) over the persistent DFS kernel.
+//
+// Host-side replacement for cuda_n_queens (src/n_queens_cuda.cu:84-186) on one
+// device.  Differences from the reference driver, all deliberate:
+//  * one device per call (no ratio split, :110-143);
+//  * device buffers and pinned staging are cached per device and grown on
+//    demand instead of cudaMalloc/cudaFree per call (:157-177);
+//  * the queue word is reset on every launch (the reference's global_counter,
+//    :8, is never reset, so its second call in a process counts nothing);
+//  * no cudaDeviceSynchronize after every call (src/macro.h:48): one stream,
+//    events for timing, one synchronisation per entry;
+//  * errors come back as nq_status codes; the library never exits.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <functional>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "dfs_kernel.cuh"
+#include "expand.h"
+#include "n_queens_b200.h"
+
+namespace nqb {
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+constexpr int kMaxBlocksPerSm = 32;
+constexpr int kDefaultThreads = 256;
+constexpr int kDefaultInner = 256;
+// d_ctl layout (uint64 words): control words, results, per-CTA partials.
+constexpr int kWordSum = kCtlWords + 0;
+constexpr int kWordNodes = kCtlWords + 1;
+constexpr int kWordStatus = kCtlWords + 2;
+constexpr int kWordBlocks = 8;
+
+thread_local std::string g_last_error;
+
+int fail_cuda(cudaError_t e, const char *what) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    (void)cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? NQ_ERR_OOM : NQ_ERR_CUDA;
+}
+
+#define NQ_CUDA(call)                                         \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return fail_cuda(e_, #call);   \
+    } while (0)
+
+double now_ms() {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+typedef void (*KernelFn)(DfsParams);
+
+KernelFn pick_kernel(bool per_owner, bool nodes) {
+    if (per_owner) return nodes ? dfs_kernel<true, true> : dfs_kernel<true, false>;
+    return nodes ? dfs_kernel<false, true> : dfs_kernel<false, false>;
+}
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    int grow(size_t need) {
+        if (need <= cap) return NQ_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(need + need / 4, 1 << 20);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc");
+        cap = want;
+        return NQ_OK;
+    }
+};
+
+struct HostBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    int grow(size_t need) {
+        if (need <= cap) return NQ_OK;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(need + need / 4, 1 << 20);
+        cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+        if (e != cudaSuccess) return fail_cuda(e, "cudaHostAlloc");
+        cap = want;
+        return NQ_OK;
+    }
+};
+
+struct Ctx {
+    std::mutex mu;
+    bool ready = false;
+    int dev = 0;
+    int sms = 0;
+    int smem_optin = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {};
+    unsigned long long *d_ctl = nullptr;  // control words + results + per-CTA partials
+    DevBuf tasks;                         // cols | ld | rd (uint32 SoA)
+    DevBuf aux;                           // order, owners, task_n, per-task outputs
+    HostBuf h_tasks;                      // pinned staging for the expander
+};
+
+Ctx g_ctx[kMaxDevices];
+
+int ensure_ready(Ctx &c, int dev) {
+    if (c.ready) {
+        NQ_CUDA(cudaSetDevice(dev));
+        return NQ_OK;
+    }
+    NQ_CUDA(cudaSetDevice(dev));
+    cudaDeviceProp prop;
+    NQ_CUDA(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major != 10 || prop.minor != 0) {
+        g_last_error = std::string("device is sm_") + std::to_string(prop.major) + std::to_string(prop.minor) +
+                       "; this library carries only an sm_100a image";
+        return NQ_ERR_NO_KERNEL;
+    }
+    c.dev = dev;
+    c.sms = prop.multiProcessorCount;
+    c.smem_optin = (int)prop.sharedMemPerBlockOptin;
+    NQ_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    for (auto &e : c.ev) NQ_CUDA(cudaEventCreate(&e));
+    const size_t ctl_words = kWordBlocks + 2 * (size_t)c.sms * kMaxBlocksPerSm;
+    NQ_CUDA(cudaMalloc(&c.d_ctl, ctl_words * sizeof(unsigned long long)));
+    NQ_CUDA(cudaMemset(c.d_ctl, 0, ctl_words * sizeof(unsigned long long)));
+    // Dynamic shared memory above 48 KiB needs an opt-in per kernel.
+    const int static_smem = 2 * 32 * 8 + 16;
+    for (int po = 0; po < 2; ++po)
+        for (int nd = 0; nd < 2; ++nd)
+            NQ_CUDA(cudaFuncSetAttribute(pick_kernel(po, nd), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         c.smem_optin - static_smem));
+    c.ready = true;
+    return NQ_OK;
+}
+
+int device_of(const nq_config *cfg) { return cfg ? cfg->device : 0; }
+
+int lock_device(int dev, Ctx *&out) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        (void)cudaGetLastError();
+        g_last_error = "no CUDA device";
+        return NQ_ERR_NO_DEVICE;
+    }
+    if (dev < 0 || dev >= n || dev >= kMaxDevices) {
+        g_last_error = "device ordinal out of range";
+        return NQ_ERR_ARG;
+    }
+    out = &g_ctx[dev];
+    return NQ_OK;
+}
+
+struct Launch {
+    int threads = 0, levels = 0, smem = 0, grid = 0, inner = 0, steal = 1;
+};
+
+// Chooses the persistent grid: CTA size, stack slots per lane and as many
+// resident CTAs per SM as shared memory and registers allow.
+int plan_launch(Ctx &c, const nq_config *cfg, int levels_needed, bool per_owner, bool nodes, Launch &L) {
+    L.threads = (cfg && cfg->block_threads) ? cfg->block_threads : kDefaultThreads;
+    if (L.threads < 32 || L.threads > 1024 || (L.threads & 31)) {
+        g_last_error = "block_threads must be a multiple of 32 in [32, 1024]";
+        return NQ_ERR_ARG;
+    }
+    L.levels = std::max(1, levels_needed);
+    if (cfg && cfg->stack_levels > 0) {
+        if (cfg->stack_levels < levels_needed) {
+            g_last_error = "stack_levels is below what the tasks need";
+            return NQ_ERR_DEPTH;
+        }
+        L.levels = cfg->stack_levels;
+    }
+    L.smem = (L.threads / 32) * L.levels * (int)kSlotBytes;
+    const int static_smem = 2 * 32 * 8 + 16;
+    if (L.smem + static_smem > c.smem_optin) {
+        g_last_error = "per-CTA stack does not fit in shared memory: lower block_threads";
+        return NQ_ERR_DEPTH;
+    }
+    int per_sm = 0;
+    NQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_kernel(per_owner, nodes), L.threads,
+                                                          L.smem));
+    if (per_sm <= 0) {
+        g_last_error = "launch configuration cannot be resident";
+        return NQ_ERR_ARG;
+    }
+    per_sm = std::min(per_sm, kMaxBlocksPerSm);
+    if (cfg && cfg->blocks_per_sm > 0) per_sm = std::min(per_sm, cfg->blocks_per_sm);
+    L.grid = c.sms * per_sm;
+    L.inner = (cfg && cfg->inner_steps > 0) ? ((cfg->inner_steps + 3) & ~3) : kDefaultInner;
+    L.steal = (cfg && cfg->steal < 0) ? 0 : 1;
+    return NQ_OK;
+}
+
+void fill_stats_launch(nq_stats *st, const Launch &L) {
+    if (!st) return;
+    st->grid = L.grid;
+    st->block_threads = L.threads;
+    st->stack_levels = L.levels;
+    st->smem_bytes = L.smem;
+}
+
+// Enqueues queue reset + kernel on stream s.
+int enqueue_dfs(Ctx &c, DfsParams p, const Launch &L, bool per_owner, bool nodes, cudaStream_t s) {
+    p.levels = L.levels;
+    p.inner = L.inner;
+    p.steal = L.steal;
+    NQ_CUDA(cudaMemsetAsync(p.ctl, 0, kCtlWords * sizeof(unsigned long long), s));
+    pick_kernel(per_owner, nodes)<<<L.grid, L.threads, L.smem, s>>>(p);
+    NQ_CUDA(cudaGetLastError());
+    return NQ_OK;
+}
+
+DfsParams base_params(Ctx &c, int N, int64_t n, const nq_config *cfg) {
+    DfsParams p;
+    memset(&p, 0, sizeof(p));
+    p.N = N;
+    p.ntasks = n;
+    p.limit_ns = cfg ? (unsigned long long)cfg->time_limit_ms * 1000000ull : 0ull;
+    p.ctl = c.d_ctl;
+    p.sum_out = c.d_ctl + kWordSum;
+    p.nodes_out = c.d_ctl + kWordNodes;
+    p.status_out = c.d_ctl + kWordStatus;
+    p.block_cnt = c.d_ctl + kWordBlocks;
+    p.block_nodes = c.d_ctl + kWordBlocks + (size_t)c.sms * kMaxBlocksPerSm;
+    return p;
+}
+
+int status_from_bits(unsigned long long bits) {
+    if (bits & kStatDepth) {
+        g_last_error = "a task needed more stack levels than the launch provided";
+        return NQ_ERR_DEPTH;
+    }
+    if (bits & kStatTimeout) {
+        g_last_error = "the kernel reached its time limit; counts are partial";
+        return NQ_ERR_TIMEOUT;
+    }
+    return NQ_OK;
+}
+
+int levels_for_tasks(int N, const uint32_t *cols, int64_t n) {
+    const uint32_t last = (N >= 32) ? 0xffffffffu : ((1u << N) - 1u);
+    int need = 1;
+    for (int64_t i = 0; i < n; ++i) {
+        const uint32_t c = cols[i];
+        if ((c & ~last) || c == last) continue;
+        need = std::max(need, N - 1 - __builtin_popcount(c));
+    }
+    return need;
+}
+
+// Counts tasks that are already in device memory (d_cols, d_ld, d_rd) and
+// downloads the results.  Used by nq_count and nq_count_tasks.
+int count_resident(Ctx &c, int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd, int64_t n,
+                   int levels_needed, const nq_config *cfg, bool per_owner, bool nodes, uint64_t *h_per_task,
+                   uint64_t *h_nodes_task, uint64_t *sum, uint64_t *nodes_total, nq_stats *st, bool timed_h2d) {
+    Launch L;
+    int rc = plan_launch(c, cfg, levels_needed, per_owner, nodes, L);
+    if (rc) return rc;
+    fill_stats_launch(st, L);
+    DfsParams p = base_params(c, N, n, cfg);
+    p.cols = d_cols;
+    p.ld = d_ld;
+    p.rd = d_rd;
+    // aux layout: [order u32 n] [out_cnt u64 n] [out_nodes u64 n]
+    size_t off_order = 0, off_cnt = 0, off_nodes = 0, need = 0;
+    const bool given = cfg && cfg->order_kind == NQ_ORDER_GIVEN && cfg->order;
+    if (given) {
+        off_order = need;
+        need += ((size_t)n * 4 + 255) & ~(size_t)255;
+    }
+    if (per_owner) {
+        off_cnt = need;
+        need += (size_t)n * 8;
+        if (nodes) {
+            off_nodes = need;
+            need += (size_t)n * 8;
+        }
+    }
+    if (need) {
+        rc = c.aux.grow(need);
+        if (rc) return rc;
+    }
+    char *aux = (char *)c.aux.p;
+    if (given) {
+        NQ_CUDA(cudaMemcpyAsync(aux + off_order, cfg->order, (size_t)n * 4, cudaMemcpyHostToDevice, c.stream));
+        p.order = (const uint32_t *)(aux + off_order);
+    }
+    if (per_owner) {
+        p.out_cnt = (unsigned long long *)(aux + off_cnt);
+        NQ_CUDA(cudaMemsetAsync(p.out_cnt, 0, (size_t)n * 8, c.stream));
+        if (nodes) {
+            p.out_nodes = (unsigned long long *)(aux + off_nodes);
+            NQ_CUDA(cudaMemsetAsync(p.out_nodes, 0, (size_t)n * 8, c.stream));
+        }
+    }
+    NQ_CUDA(cudaEventRecord(c.ev[1], c.stream));
+    rc = enqueue_dfs(c, p, L, per_owner, nodes, c.stream);
+    if (rc) return rc;
+    NQ_CUDA(cudaEventRecord(c.ev[2], c.stream));
+    unsigned long long res[3] = {0, 0, 0};
+    NQ_CUDA(cudaMemcpyAsync(res, c.d_ctl + kWordSum, sizeof(res), cudaMemcpyDeviceToHost, c.stream));
+    if (per_owner && h_per_task)
+        NQ_CUDA(cudaMemcpyAsync(h_per_task, p.out_cnt, (size_t)n * 8, cudaMemcpyDeviceToHost, c.stream));
+    if (per_owner && nodes && h_nodes_task)
+        NQ_CUDA(cudaMemcpyAsync(h_nodes_task, p.out_nodes, (size_t)n * 8, cudaMemcpyDeviceToHost, c.stream));
+    NQ_CUDA(cudaEventRecord(c.ev[3], c.stream));
+    NQ_CUDA(cudaStreamSynchronize(c.stream));
+    if (st) {
+        float ms = 0;
+        if (timed_h2d) {
+            cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]);
+            st->h2d_ms = ms;
+        }
+        cudaEventElapsedTime(&ms, c.ev[1], c.ev[2]);
+        st->kernel_ms = ms;
+        cudaEventElapsedTime(&ms, c.ev[2], c.ev[3]);
+        st->d2h_ms = ms;
+        if (nodes) st->nodes = res[1];
+    }
+    if (sum) *sum = res[0];
+    if (nodes_total) *nodes_total = res[1];
+    return status_from_bits(res[2]);
+}
+
+}  // namespace
+
+}  // namespace nqb
+
+using namespace nqb;
+
+extern "C" {
+
+int nq_abi_version(void) { return NQ_ABI_VERSION; }
+
+const char *nq_status_string(int status) {
+    switch (status) {
+        case NQ_OK: return "ok";
+        case NQ_ERR_ARG: return "invalid argument";
+        case NQ_ERR_NO_DEVICE: return "no CUDA device";
+        case NQ_ERR_CUDA: return "CUDA runtime error";
+        case NQ_ERR_OOM: return "out of memory";
+        case NQ_ERR_DEPTH: return "stack depth exceeds the launch's stack";
+        case NQ_ERR_TIMEOUT: return "time limit reached; counts are partial";
+        case NQ_ERR_NO_KERNEL: return "no kernel image for this device";
+        default: return "unknown status";
+    }
+}
+
+const char *nq_last_error(void) { return g_last_error.c_str(); }
+
+int nq_device_count(int *count) {
+    if (!count) return NQ_ERR_ARG;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) {
+        (void)cudaGetLastError();
+        *count = 0;
+        return NQ_OK;
+    }
+    if (e != cudaSuccess) {
+        *count = 0;
+        return fail_cuda(e, "cudaGetDeviceCount");
+    }
+    *count = n;
+    return NQ_OK;
+}
+
+int nq_expand(int N, int rows, uint32_t *cols, uint32_t *ld, uint32_t *rd, int64_t cap, int64_t *n_tasks,
+              int threads) {
+    if (N < 2 || N > NQ_MAX_N || rows < 1 || rows > N || !n_tasks || cap < 0) return NQ_ERR_ARG;
+    if (cap > 0 && (!cols || !ld || !rd)) return NQ_ERR_ARG;
+    const int64_t n = expand_prefixes(N, rows, cols, ld, rd, cap, threads);
+    if (n < 0) return NQ_ERR_ARG;
+    *n_tasks = n;
+    return NQ_OK;
+}
+
+int nq_count(int N, int rows, const nq_config *cfg, uint64_t *total, uint64_t *nodes, nq_stats *stats) {
+    const double t0 = now_ms();
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (N < 2 || N > NQ_MAX_N || rows < 1 || rows > N - 2 || !total) return NQ_ERR_ARG;
+    Ctx *cp = nullptr;
+    int rc = lock_device(device_of(cfg), cp);
+    if (rc == NQ_ERR_NO_DEVICE) {
+        // Mirror the reference: the prefixes are generated before the GPU
+        // count is checked (src/n_queens_cuda.cu:91-108).
+        const double te = now_ms();
+        const int64_t n = expand_prefixes(N, rows, nullptr, nullptr, nullptr, 0, 0);
+        if (stats) {
+            stats->expand_ms = now_ms() - te;
+            stats->tasks = n;
+            stats->total_ms = now_ms() - t0;
+        }
+        return rc;
+    }
+    if (rc) return rc;
+    Ctx &c = *cp;
+    std::lock_guard<std::mutex> lock(c.mu);
+    rc = ensure_ready(c, device_of(cfg));
+    if (rc) return rc;
+
+    const double te = now_ms();
+    uint32_t *h = nullptr;
+    int grow_rc = NQ_OK;
+    const int64_t n = expand_prefixes_to(
+        N, rows,
+        [&](int64_t total_tasks, uint32_t **pc, uint32_t **pl, uint32_t **pr, int64_t *cap) {
+            grow_rc = c.h_tasks.grow((size_t)std::max<int64_t>(total_tasks, 1) * 12);
+            if (grow_rc) return false;
+            h = (uint32_t *)c.h_tasks.p;
+            *pc = h;
+            *pl = h + total_tasks;
+            *pr = h + 2 * total_tasks;
+            *cap = total_tasks;
+            return true;
+        },
+        0);
+    if (grow_rc) return grow_rc;
+    if (n < 0) return NQ_ERR_ARG;
+    if (stats) {
+        stats->expand_ms = now_ms() - te;
+        stats->tasks = n;
+    }
+    rc = c.tasks.grow((size_t)std::max<int64_t>(n, 1) * 12);
+    if (rc) return rc;
+    uint32_t *d = (uint32_t *)c.tasks.p;
+    NQ_CUDA(cudaEventRecord(c.ev[0], c.stream));
+    if (n) NQ_CUDA(cudaMemcpyAsync(d, h, (size_t)n * 12, cudaMemcpyHostToDevice, c.stream));
+    uint64_t sum = 0, nd = 0;
+    rc = count_resident(c, N, d, d + n, d + 2 * n, n, N - 1 - rows, cfg, false, nodes != nullptr, nullptr, nullptr,
+                        &sum, &nd, stats, true);
+    // The reference doubles every per-prefix sum for the mirror image
+    // (src/n_queens_cuda.cu:181-183).
+    *total = 2 * sum;
+    if (nodes) *nodes = nd;
+    if (stats) stats->total_ms = now_ms() - t0;
+    return rc;
+}
+
+int nq_count_tasks(int N, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd, int64_t n,
+                   uint64_t *per_task, uint64_t *nodes_per_task, uint64_t *sum, const nq_config *cfg,
+                   nq_stats *stats) {
+    const double t0 = now_ms();
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (N < 1 || N > NQ_MAX_N || n < 0 || !sum) return NQ_ERR_ARG;
+    if (n > 0 && (!cols || !ld || !rd)) return NQ_ERR_ARG;
+    if (n > 0xffffffffll) return NQ_ERR_ARG;
+    Ctx *cp = nullptr;
+    int rc = lock_device(device_of(cfg), cp);
+    if (rc) return rc;
+    Ctx &c = *cp;
+    std::lock_guard<std::mutex> lock(c.mu);
+    rc = ensure_ready(c, device_of(cfg));
+    if (rc) return rc;
+    if (stats) stats->tasks = n;
+    if (n == 0) {
+        *sum = 0;
+        if (stats) stats->total_ms = now_ms() - t0;
+        return NQ_OK;
+    }
+    const int need = levels_for_tasks(N, cols, n);
+    rc = c.tasks.grow((size_t)n * 12);
+    if (rc) return rc;
+    uint32_t *d = (uint32_t *)c.tasks.p;
+    NQ_CUDA(cudaEventRecord(c.ev[0], c.stream));
+    NQ_CUDA(cudaMemcpyAsync(d, cols, (size_t)n * 4, cudaMemcpyHostToDevice, c.stream));
+    NQ_CUDA(cudaMemcpyAsync(d + n, ld, (size_t)n * 4, cudaMemcpyHostToDevice, c.stream));
+    NQ_CUDA(cudaMemcpyAsync(d + 2 * n, rd, (size_t)n * 4, cudaMemcpyHostToDevice, c.stream));
+    const bool per_owner = per_task != nullptr || nodes_per_task != nullptr;
+    const bool want_nodes = nodes_per_task != nullptr;
+    std::vector<uint64_t> tmp;
+    uint64_t *pt = per_task;
+    if (per_owner && !pt) {
+        tmp.resize((size_t)n);
+        pt = tmp.data();
+    }
+    rc = count_resident(c, N, d, d + n, d + 2 * n, n, need, cfg, per_owner, want_nodes, pt, nodes_per_task, sum,
+                        nullptr, stats, true);
+    if (stats) stats->total_ms = now_ms() - t0;
+    return rc;
+}
+
+int nq_count_tasks_device(int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd, int64_t n,
+                          uint64_t *d_per_task, uint64_t *d_nodes, uint64_t *d_sum, const nq_config *cfg,
+                          void *stream) {
+    if (N < 1 || N > NQ_MAX_N || n < 0 || !d_sum) return NQ_ERR_ARG;
+    if (n > 0 && (!d_cols || !d_ld || !d_rd)) return NQ_ERR_ARG;
+    if (n > 0xffffffffll) return NQ_ERR_ARG;
+    if (d_nodes && !d_per_task) return NQ_ERR_ARG;
+    Ctx *cp = nullptr;
+    int rc = lock_device(device_of(cfg), cp);
+    if (rc) return rc;
+    Ctx &c = *cp;
+    std::lock_guard<std::mutex> lock(c.mu);
+    rc = ensure_ready(c, device_of(cfg));
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    // Without a host view of the tasks the stack must cover the deepest
+    // possible task (an empty board) unless the caller states the depth.
+    const int need = (cfg && cfg->stack_levels > 0) ? cfg->stack_levels : N - 1;
+    const bool per_owner = d_per_task != nullptr;
+    const bool want_nodes = d_nodes != nullptr;
+    Launch L;
+    rc = plan_launch(c, cfg, need, per_owner, want_nodes, L);
+    if (rc) return rc;
+    DfsParams p = base_params(c, N, n, cfg);
+    p.cols = d_cols;
+    p.ld = d_ld;
+    p.rd = d_rd;
+    p.sum_out = (unsigned long long *)d_sum;
+    p.status_out = (unsigned long long *)d_sum + 1;
+    if (cfg && cfg->order_kind == NQ_ORDER_GIVEN && cfg->order) p.order = cfg->order;
+    if (per_owner) {
+        p.out_cnt = (unsigned long long *)d_per_task;
+        NQ_CUDA(cudaMemsetAsync(d_per_task, 0, (size_t)n * 8, s));
+        if (want_nodes) {
+            p.out_nodes = (unsigned long long *)d_nodes;
+            NQ_CUDA(cudaMemsetAsync(d_nodes, 0, (size_t)n * 8, s));
+        }
+    }
+    return enqueue_dfs(c, p, L, per_owner, want_nodes, s);
+}
+
+int nq_count_batch(const nq_instance *inst, int64_t n, int split_rows, uint64_t *out, const nq_config *cfg,
+                   nq_stats *stats) {
+    const double t0 = now_ms();
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (n < 0 || (n > 0 && (!inst || !out)) || split_rows < 0 || split_rows > 8) return NQ_ERR_ARG;
+    if (n > 0xffffffffll) return NQ_ERR_ARG;
+    for (int64_t i = 0; i < n; ++i)
+        if (inst[i].N < 1 || inst[i].N > NQ_MAX_N) return NQ_ERR_ARG;
+    Ctx *cp = nullptr;
+    int rc = lock_device(device_of(cfg), cp);
+    if (rc) return rc;
+    Ctx &c = *cp;
+    std::lock_guard<std::mutex> lock(c.mu);
+    rc = ensure_ready(c, device_of(cfg));
+    if (rc) return rc;
+    if (n == 0) return NQ_OK;
+    const int split = split_rows ? split_rows : 3;
+
+    // Split every instance into subtasks; a subtask remembers its instance
+    // (owner) and board size.
+    const double te = now_ms();
+    std::vector<uint32_t> tc, tl, tr, own;
+    std::vector<uint8_t> tn;
+    int need = 1;
+    for (int64_t i = 0; i < n; ++i) {
+        const int N = inst[i].N;
+        const size_t before = tc.size();
+        expand_board(N, inst[i].cols, inst[i].ld, inst[i].rd, split, tc, tl, tr);
+        const uint32_t last = (N >= 32) ? 0xffffffffu : ((1u << N) - 1u);
+        for (size_t k = before; k < tc.size(); ++k) {
+            own.push_back((uint32_t)i);
+            tn.push_back((uint8_t)N);
+            if (!(tc[k] & ~last) && tc[k] != last) need = std::max(need, N - 1 - __builtin_popcount(tc[k]));
+        }
+    }
+    const int64_t m = (int64_t)tc.size();
+    if (stats) {
+        stats->expand_ms = now_ms() - te;
+        stats->tasks = m;
+    }
+    // tasks: cols | ld | rd | owner (u32 each), then task_n (u8)
+    rc = c.tasks.grow((size_t)m * 17 + 256);
+    if (rc) return rc;
+    uint32_t *d = (uint32_t *)c.tasks.p;
+    NQ_CUDA(cudaEventRecord(c.ev[0], c.stream));
+    if (m) {
+        NQ_CUDA(cudaMemcpyAsync(d, tc.data(), (size_t)m * 4, cudaMemcpyHostToDevice, c.stream));
+        NQ_CUDA(cudaMemcpyAsync(d + m, tl.data(), (size_t)m * 4, cudaMemcpyHostToDevice, c.stream));
+        NQ_CUDA(cudaMemcpyAsync(d + 2 * m, tr.data(), (size_t)m * 4, cudaMemcpyHostToDevice, c.stream));
+        NQ_CUDA(cudaMemcpyAsync(d + 3 * m, own.data(), (size_t)m * 4, cudaMemcpyHostToDevice, c.stream));
+        NQ_CUDA(cudaMemcpyAsync(d + 4 * m, tn.data(), (size_t)m, cudaMemcpyHostToDevice, c.stream));
+    }
+    Launch L;
+    rc = plan_launch(c, cfg, need, true, false, L);
+    if (rc) return rc;
+    fill_stats_launch(stats, L);
+    rc = c.aux.grow((size_t)n * 8);
+    if (rc) return rc;
+    DfsParams p = base_params(c, 0, m, cfg);
+    p.cols = d;
+    p.ld = d + m;
+    p.rd = d + 2 * m;
+    p.owner_of = d + 3 * m;
+    p.task_n = (const uint8_t *)(d + 4 * m);
+    p.out_cnt = (unsigned long long *)c.aux.p;
+    NQ_CUDA(cudaMemsetAsync(p.out_cnt, 0, (size_t)n * 8, c.stream));
+    NQ_CUDA(cudaEventRecord(c.ev[1], c.stream));
+    rc = enqueue_dfs(c, p, L, true, false, c.stream);
+    if (rc) return rc;
+    NQ_CUDA(cudaEventRecord(c.ev[2], c.stream));
+    unsigned long long res[3] = {0, 0, 0};
+    NQ_CUDA(cudaMemcpyAsync(res, c.d_ctl + kWordSum, sizeof(res), cudaMemcpyDeviceToHost, c.stream));
+    NQ_CUDA(cudaMemcpyAsync(out, p.out_cnt, (size_t)n * 8, cudaMemcpyDeviceToHost, c.stream));
+    NQ_CUDA(cudaEventRecord(c.ev[3], c.stream));
+    NQ_CUDA(cudaStreamSynchronize(c.stream));
+    if (stats) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]);
+        stats->h2d_ms = ms;
+        cudaEventElapsedTime(&ms, c.ev[1], c.ev[2]);
+        stats->kernel_ms = ms;
+        cudaEventElapsedTime(&ms, c.ev[2], c.ev[3]);
+        stats->d2h_ms = ms;
+        stats->total_ms = now_ms() - t0;
+    }
+    return status_from_bits(res[2]);
+}
+
+}  // extern "C"

@@ -1,0 +1,435 @@
+// dfs_kernel.cuh -- persistent iterative-DFS kernel for sm_100a.
+//
+// Replaces the reference kernel n_queens() of src/n_queens_cuda.cu:9-82 and
+// its ticket counter global_counter (:8).  Same per-task arithmetic
+// (n_queens() of src/n_queens.cpp:8-21); different machine organisation:
+//
+//  * One lane runs one DFS.  The current level lives in registers
+//    (cols, ld, rd, avail); only levels that still have untried columns are
+//    pushed to the lane's shared-memory stack, so a pop always resumes a level
+//    with work and every DFS step places exactly one queen.
+//  * cols carries the off-board bits (~last) pre-set.  Then the free mask is
+//    one LOP3 (~(cols|ld|rd)) with no `& last`, a completed board is
+//    cols == 0xffffffff, and no depth counter is kept at all.
+//  * Stack layout: slot s of lane l in warp w is the 16-byte entry at
+//    w*levels*512 + s*512 + l*16.  Every stack access is a 128-bit LDS/STS and
+//    a quarter-warp always covers 128 contiguous bytes whatever the per-lane
+//    depths are, so no access has a bank conflict (the reference mixes in a
+//    32-bit store, src/n_queens_cuda.cu:47, which is 4-way conflicted).
+//  * Tasks come from a device queue: one atomicAdd per warp refill hands a
+//    block of consecutive queue positions to the idle lanes (the reference
+//    takes one atomic per task per thread, :10,80).  An optional permutation
+//    maps queue positions to tasks (longest-first schedules).
+//  * Once the queue is empty, idle lanes take the bottom (shallowest, hence
+//    largest) stacked level of a busy lane in the same warp: __ballot_sync
+//    finds donors and receivers, __shfl_sync moves the donor's slot address,
+//    and the receiver loads the entry straight from the donor's stack.
+//  * Counts are uint32 per lane inside a bounded inner loop, folded into
+//    uint64 per lane, reduced per warp (shuffles) and per CTA, and the last
+//    CTA to finish sums the per-CTA partials in a fixed order.
+//
+// The kernel has no spin-wait of any kind: a lane never waits for another
+// CTA or for host memory.  An optional %globaltimer deadline bounds its run.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace nqb {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kSlotBytes = 512;  // one stack level of one warp: 32 lanes x 16 B
+constexpr uint32_t kNoOwner = 0xffffffffu;
+
+enum CtlWord : int {
+    kCtlHead = 0,      // next queue position
+    kCtlDone = 1,      // CTAs finished
+    kCtlError = 2,     // error bits (kErr*)
+    kCtlTimeout = 3,   // set when the deadline stopped the kernel
+    kCtlWords = 4,
+};
+enum : unsigned long long { kErrDepth = 1ull };
+// Bits of *status_out: a task needed more stack levels than the launch had
+// (it was skipped), and/or the run-time limit stopped the kernel early.
+enum : unsigned long long { kStatDepth = 1ull, kStatTimeout = 2ull };
+
+struct DfsParams {
+    const uint32_t *cols;      // task column masks (reference `cur`)
+    const uint32_t *ld;        // task left-diagonal masks (reference `left`)
+    const uint32_t *rd;        // task right-diagonal masks (reference `right`)
+    const uint8_t *task_n;     // per-task board size, or nullptr (use N)
+    const uint32_t *owner_of;  // per-task output slot, or nullptr (slot = task index)
+    const uint32_t *order;     // queue position -> task index, or nullptr (identity)
+    long long ntasks;
+    int N;                     // board size when task_n is nullptr
+    int levels;                // stack slots per lane
+    int inner;                 // DFS steps per outer trip (multiple of 4)
+    int steal;                 // in-warp donation on/off
+    unsigned long long limit_ns;     // run-time limit from the CTA's start, 0 = none
+    unsigned long long *ctl;         // kCtlWords control words (zeroed before launch)
+    unsigned long long *block_cnt;   // [gridDim.x] per-CTA count partials
+    unsigned long long *block_nodes; // [gridDim.x] per-CTA node partials (NODES)
+    unsigned long long *out_cnt;     // per-owner counts (PER_OWNER), zeroed by the host
+    unsigned long long *out_nodes;   // per-owner nodes (PER_OWNER && NODES), zeroed by the host
+    unsigned long long *sum_out;     // total count (device word)
+    unsigned long long *nodes_out;   // total nodes (device word, NODES)
+    unsigned long long *status_out;  // kStat* bits of this launch (device word)
+};
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uint32_t &z, uint32_t &w) {
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(x), "=r"(y), "=r"(z), "=r"(w) : "r"(a) : "memory");
+}
+
+// One DFS step of one lane, branch-free.  State: (cols, ld, rd, avail) of the
+// level being enumerated; sp/bot are the lane's stack top/bottom addresses.
+//   bit   = lowest free column;  avail -= bit
+//   child = (cols|bit, (ld|bit)<<1, (rd|bit)>>1),  free = ~(c|l|r)
+//   child cols == ~0            -> one completed board: cnt += 1
+//   free != 0 (and bit != 0)    -> descend; the parent is pushed only if
+//                                  it still has untried columns
+//   otherwise, level exhausted  -> pop a stacked level if there is one
+// An idle lane (avail == 0, empty stack) passes through with no effect.
+// Right shift is arithmetic, as in the reference's `int` arithmetic.
+#define NQB_STEP_ASM                                                                  \
+    "{\n\t"                                                                           \
+    ".reg .pred pb, pd, pp, pe, pq;\n\t"                                              \
+    ".reg .b32 bit, nc, nl, nr, na;\n\t"                                              \
+    "neg.s32 bit, %3;\n\t"                                                            \
+    "and.b32 bit, bit, %3;\n\t"                                                       \
+    "xor.b32 %3, %3, bit;\n\t"                                                        \
+    "or.b32 nc, %0, bit;\n\t"                                                         \
+    "or.b32 nl, %1, bit;\n\t"                                                         \
+    "shl.b32 nl, nl, 1;\n\t"                                                          \
+    "or.b32 nr, %2, bit;\n\t"                                                         \
+    "shr.s32 nr, nr, 1;\n\t"                                                          \
+    "lop3.b32 na, nc, nl, nr, 0x01;\n\t"                                              \
+    "setp.eq.u32 pe, nc, 0xffffffff;\n\t"                                             \
+    "@pe add.u32 %5, %5, 1;\n\t"                                                      \
+    "setp.ne.u32 pb, bit, 0;\n\t"                                                     \
+    "setp.ne.and.u32 pd, na, 0, pb;\n\t"                                              \
+    "setp.ne.and.u32 pp, %3, 0, pd;\n\t"                                              \
+    "@pp st.shared.v4.u32 [%4], {%0, %1, %2, %3};\n\t"                                \
+    "@pp add.u32 %4, %4, 512;\n\t"                                                    \
+    "@pd mov.b32 %0, nc;\n\t"                                                         \
+    "@pd mov.b32 %1, nl;\n\t"                                                         \
+    "@pd mov.b32 %2, nr;\n\t"                                                         \
+    "@pd mov.b32 %3, na;\n\t"                                                         \
+    "setp.eq.u32 pq, %3, 0;\n\t"                                                      \
+    "setp.ne.and.u32 pq, %4, %6, pq;\n\t"                                             \
+    "@pq sub.u32 %4, %4, 512;\n\t"                                                    \
+    "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"                                \
+    "}\n\t"
+
+// Same step, also counting placements (for the node statistics).
+#define NQB_STEP_ASM_NODES                                                            \
+    "{\n\t"                                                                           \
+    ".reg .pred pb, pd, pp, pe, pq;\n\t"                                              \
+    ".reg .b32 bit, nc, nl, nr, na;\n\t"                                              \
+    "neg.s32 bit, %3;\n\t"                                                            \
+    "and.b32 bit, bit, %3;\n\t"                                                       \
+    "xor.b32 %3, %3, bit;\n\t"                                                        \
+    "or.b32 nc, %0, bit;\n\t"                                                         \
+    "or.b32 nl, %1, bit;\n\t"                                                         \
+    "shl.b32 nl, nl, 1;\n\t"                                                          \
+    "or.b32 nr, %2, bit;\n\t"                                                         \
+    "shr.s32 nr, nr, 1;\n\t"                                                          \
+    "lop3.b32 na, nc, nl, nr, 0x01;\n\t"                                              \
+    "setp.eq.u32 pe, nc, 0xffffffff;\n\t"                                             \
+    "@pe add.u32 %5, %5, 1;\n\t"                                                      \
+    "setp.ne.u32 pb, bit, 0;\n\t"                                                     \
+    "@pb add.u32 %6, %6, 1;\n\t"                                                      \
+    "setp.ne.and.u32 pd, na, 0, pb;\n\t"                                              \
+    "setp.ne.and.u32 pp, %3, 0, pd;\n\t"                                              \
+    "@pp st.shared.v4.u32 [%4], {%0, %1, %2, %3};\n\t"                                \
+    "@pp add.u32 %4, %4, 512;\n\t"                                                    \
+    "@pd mov.b32 %0, nc;\n\t"                                                         \
+    "@pd mov.b32 %1, nl;\n\t"                                                         \
+    "@pd mov.b32 %2, nr;\n\t"                                                         \
+    "@pd mov.b32 %3, na;\n\t"                                                         \
+    "setp.eq.u32 pq, %3, 0;\n\t"                                                      \
+    "setp.ne.and.u32 pq, %4, %7, pq;\n\t"                                             \
+    "@pq sub.u32 %4, %4, 512;\n\t"                                                    \
+    "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"                                \
+    "}\n\t"
+
+template <bool NODES>
+struct Step;
+
+template <>
+struct Step<false> {
+    static __device__ __forceinline__ void run(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail,
+                                               uint32_t &sp, uint32_t &cnt, uint32_t bot, uint32_t &) {
+        asm volatile(NQB_STEP_ASM
+                     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt)
+                     : "r"(bot)
+                     : "memory");
+    }
+};
+
+template <>
+struct Step<true> {
+    static __device__ __forceinline__ void run(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail,
+                                               uint32_t &sp, uint32_t &cnt, uint32_t bot, uint32_t &it) {
+        asm volatile(NQB_STEP_ASM_NODES
+                     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
+                     : "r"(bot)
+                     : "memory");
+    }
+};
+
+// Loads task t into a lane.  Returns the completions credited immediately
+// (1 for an already-complete board) and leaves avail == 0 when the task has
+// no free column.  A column mask with off-board bits can never equal `last`,
+// so such a task counts 0, exactly as the reference recursion does.
+__device__ __forceinline__ uint32_t load_task(const DfsParams &p, long long t, uint32_t &cols, uint32_t &ld,
+                                              uint32_t &rd, uint32_t &avail) {
+    const int n = p.task_n ? (int)p.task_n[t] : p.N;
+    const uint32_t last = (n >= 32) ? kFull : ((1u << n) - 1u);
+    const uint32_t c = __ldg(p.cols + t);
+    const uint32_t l = __ldg(p.ld + t);
+    const uint32_t r = __ldg(p.rd + t);
+    avail = 0;
+    if (c & ~last) return 0;
+    if (c == last) return 1;
+    // Stack slots this task can use: one per level that still has a sibling,
+    // at most N-1-popc(cols).
+    const int need = n - 1 - __popc(c);
+    if (need > p.levels) {
+        atomicOr(p.ctl + kCtlError, kErrDepth);
+        return 0;
+    }
+    cols = c | ~last;
+    ld = l;
+    rd = r;
+    avail = ~(cols | l | r);
+    return 0;
+}
+
+template <bool PER_OWNER, bool NODES>
+__global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ unsigned long long red_cnt[32];
+    __shared__ unsigned long long red_nodes[32];
+    __shared__ int s_is_last;
+
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t smem_base = (uint32_t)__cvta_generic_to_shared(smem_raw);
+    const uint32_t my_base = smem_base + warp * (uint32_t)p.levels * kSlotBytes + lane * 16u;
+
+    uint32_t cols = 0, ld = 0, rd = 0, avail = 0;
+    uint32_t sp = my_base, bot = my_base;
+    uint32_t cnt = 0, it = 0;
+    uint32_t owner = kNoOwner;
+    unsigned long long tot = 0, tot_nodes = 0;
+    bool queue_live = true;
+    unsigned long long deadline = 0;
+    if (p.limit_ns) {
+        unsigned long long t0 = 0;
+        if (lane == 0) t0 = globaltimer_ns();
+        deadline = __shfl_sync(kFull, t0, 0) + p.limit_ns;
+    }
+
+    for (;;) {
+        // ---- fold the per-lane 32-bit counters (bounded inner loop keeps them < 2^32)
+        if (PER_OWNER) {
+            if (avail == 0 && owner != kNoOwner) {
+                if (cnt) atomicAdd(p.out_cnt + owner, (unsigned long long)cnt);
+                if (NODES && it) atomicAdd(p.out_nodes + owner, (unsigned long long)(it - cnt));
+                tot += cnt;
+                if (NODES) tot_nodes += it - cnt;
+                cnt = 0;
+                it = 0;
+                owner = kNoOwner;
+            }
+        } else {
+            tot += cnt;
+            if (NODES) tot_nodes += it - cnt;
+            cnt = 0;
+            it = 0;
+        }
+
+        // ---- deadline (lane 0 reads the timer; the decision is warp-uniform)
+        if (deadline) {
+            unsigned long long now = 0;
+            if (lane == 0) now = globaltimer_ns();
+            now = __shfl_sync(kFull, now, 0);
+            if (now > deadline) {
+                if (lane == 0) atomicExch(p.ctl + kCtlTimeout, 1ull);
+                break;
+            }
+        }
+
+        unsigned idle = __ballot_sync(kFull, avail == 0);
+        bool check_idle = true;
+        if (idle) {
+            if (queue_live) {
+                // ---- refill from the queue: one atomic per warp
+                const int nidle = __popc(idle);
+                const int leader = __ffs(idle) - 1;
+                unsigned long long b = 0;
+                if ((int)lane == leader) b = atomicAdd(p.ctl + kCtlHead, (unsigned long long)nidle);
+                b = __shfl_sync(kFull, b, leader);
+                if (b + (unsigned long long)nidle >= (unsigned long long)p.ntasks) queue_live = false;
+                if (avail == 0) {
+                    const unsigned long long q = b + (unsigned long long)__popc(idle & lanemask_lt());
+                    const long long t = (q < (unsigned long long)p.ntasks)
+                                            ? (p.order ? (long long)__ldg(p.order + q) : (long long)q)
+                                            : -1;
+                    // A permutation entry out of range is skipped, never dereferenced.
+                    if (t >= 0 && t < p.ntasks) {
+                        sp = bot = my_base;
+                        const uint32_t done = load_task(p, t, cols, ld, rd, avail);
+                        const uint32_t own = p.owner_of ? __ldg(p.owner_of + t) : (uint32_t)t;
+                        if (PER_OWNER) {
+                            if (done) atomicAdd(p.out_cnt + own, (unsigned long long)done);
+                            if (avail) owner = own;
+                        }
+                        tot += done;
+                    }
+                }
+                // Lanes whose task was empty are still idle: refill again.
+                if (queue_live) continue;
+                idle = __ballot_sync(kFull, avail == 0);
+            }
+            if (idle && !queue_live) {
+                if (p.steal) {
+                    // ---- in-warp donation: k-th idle lane takes the bottom
+                    // stacked level of the k-th lane that has one.
+                    const unsigned rich = __ballot_sync(kFull, sp != bot);
+                    __syncwarp();  // order the donors' earlier stack stores before the reads below
+                    const int npair = min(__popc(idle), __popc(rich));
+                    if (npair > 0) {
+                        int donor = -1;
+                        if (avail == 0) {
+                            const int k = __popc(idle & lanemask_lt());
+                            if (k < npair) {
+                                unsigned m = rich;
+                                for (int i = 0; i < k; ++i) m &= m - 1;
+                                donor = __ffs(m) - 1;
+                            }
+                        }
+                        const uint32_t src_addr = __shfl_sync(kFull, bot, donor < 0 ? lane : donor);
+                        const uint32_t src_owner = __shfl_sync(kFull, owner, donor < 0 ? lane : donor);
+                        if (donor >= 0) {
+                            lds128(src_addr, cols, ld, rd, avail);
+                            sp = bot = my_base;
+                            owner = src_owner;
+                        }
+                        __syncwarp();
+                        if (sp != bot && __popc(rich & lanemask_lt()) < npair) bot += kSlotBytes;
+                        __syncwarp();
+                    } else {
+                        // Nobody can donate right now: run a full trip
+                        // without idle checks, then look again.
+                        if (idle == kFull) break;  // whole warp idle, queue empty: done
+                        check_idle = false;
+                    }
+                } else {
+                    if (idle == kFull) break;
+                    check_idle = false;
+                }
+            }
+        }
+
+        // ---- DFS steps
+        if (check_idle) {
+            for (int s = 0; s < p.inner; s += 4) {
+                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
+                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
+                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
+                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
+                if (__any_sync(kFull, avail == 0)) break;
+            }
+        } else {
+            for (int s = 0; s < p.inner; s += 4) {
+                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
+                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
+                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
+                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
+                if (__all_sync(kFull, avail == 0)) break;
+            }
+        }
+    }
+
+    // Flush what the last trip left (deadline exit, or the final fold).
+    if (PER_OWNER) {
+        if (owner != kNoOwner) {
+            if (cnt) atomicAdd(p.out_cnt + owner, (unsigned long long)cnt);
+            if (NODES && it) atomicAdd(p.out_nodes + owner, (unsigned long long)(it - cnt));
+        }
+    }
+    tot += cnt;
+    if (NODES) tot_nodes += it - cnt;
+
+    // ---- per-warp, per-CTA reduction
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        tot += __shfl_xor_sync(kFull, tot, o);
+        if (NODES) tot_nodes += __shfl_xor_sync(kFull, tot_nodes, o);
+    }
+    if (lane == 0) {
+        red_cnt[warp] = tot;
+        red_nodes[warp] = tot_nodes;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long s = 0, sn = 0;
+        for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) {
+            s += red_cnt[w];
+            sn += red_nodes[w];
+        }
+        p.block_cnt[blockIdx.x] = s;
+        if (NODES) p.block_nodes[blockIdx.x] = sn;
+        __threadfence();
+        const unsigned long long ticket = atomicAdd(p.ctl + kCtlDone, 1ull);
+        s_is_last = (ticket == (unsigned long long)gridDim.x - 1ull);
+    }
+    __syncthreads();
+    // ---- the last CTA sums the per-CTA partials in CTA order
+    if (s_is_last) {
+        __threadfence();
+        unsigned long long s = 0, sn = 0;
+        for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+            s += *((volatile unsigned long long *)(p.block_cnt + b));
+            if (NODES) sn += *((volatile unsigned long long *)(p.block_nodes + b));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s += __shfl_xor_sync(kFull, s, o);
+            if (NODES) sn += __shfl_xor_sync(kFull, sn, o);
+        }
+        __syncthreads();
+        if (lane == 0) {
+            red_cnt[warp] = s;
+            red_nodes[warp] = sn;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long a = 0, an = 0;
+            for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) {
+                a += red_cnt[w];
+                an += red_nodes[w];
+            }
+            *p.sum_out = a;
+            if (NODES) *p.nodes_out = an;
+            const unsigned long long err = *((volatile unsigned long long *)(p.ctl + kCtlError));
+            const unsigned long long tmo = *((volatile unsigned long long *)(p.ctl + kCtlTimeout));
+            *p.status_out = ((err & kErrDepth) ? kStatDepth : 0ull) | (tmo ? kStatTimeout : 0ull);
+        }
+    }
+}
+
+}  // namespace nqb

@@ -1,0 +1,161 @@
+"""GPU parity: every count through the C ABI, bit-exact against the oracle
+(oracle/, pinned to the reference) or the reference's published totals."""
+import numpy as np
+import pytest
+
+import oracle
+from n_queens_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def test_whole_board_small_n_all_k(gpu):
+    for N in range(4, 15):
+        want = oracle.total(N, 2)
+        for k in range(1, N - 1):
+            r = gpu.count(N, k)
+            assert r.total == want, (N, k)
+
+
+def test_whole_board_published(gpu, golden):
+    pub = golden("published.json")
+    for N, k in [(13, 5), (14, 5), (15, 5), (16, 5), (16, 6), (17, 6), (18, 6), (19, 6)]:
+        assert gpu.count(N, k).total == pub[str(N)]["total"], (N, k)
+        assert gpu.cuda_n_queens(N, k) == pub[str(N)]["total"]
+
+
+def test_nodes_match_oracle(gpu):
+    table = {(12, 4): 418_515, (16, 5): 563_126_914, (16, 6): 562_707_506, (17, 6): 3_959_755_915}
+    for (N, k), nodes in table.items():
+        r = gpu.count(N, k, nodes=True)
+        assert r.nodes == nodes, (N, k)
+    for N, k in [(9, 3), (10, 4), (11, 3), (13, 5)]:
+        want_total, want_nodes = oracle.total(N, k, with_nodes=True)
+        r = gpu.count(N, k, nodes=True)
+        assert (r.total, r.nodes) == (want_total, want_nodes), (N, k)
+
+
+def test_per_task_counts_and_nodes(gpu):
+    for N, k in [(10, 3), (12, 4), (13, 5), (15, 5)]:
+        c, l, r = oracle.expand(N, k)
+        want_cnt, want_nodes = oracle.count_tasks(N, c, l, r, nodes=True)
+        res = gpu.count_tasks(N, c, l, r, per_task=True, nodes=True)
+        assert np.array_equal(res["per_task"], want_cnt), (N, k)
+        assert np.array_equal(res["nodes"], want_nodes), (N, k)
+        assert res["sum"] == int(want_cnt.sum())
+
+
+def test_per_task_golden_hashes(gpu, golden):
+    import hashlib
+    for case in golden("per_task.json"):
+        c, l, r = oracle.expand(case["N"], case["k"])
+        res = gpu.count_tasks(case["N"], c, l, r, per_task=True)
+        got = res["per_task"].astype(np.int64)
+        assert hashlib.sha256(got.tobytes()).hexdigest() == case["sha256_counts_int64"], case
+        assert 2 * res["sum"] == case["sum_x2"]
+
+
+def test_arbitrary_32bit_inputs(gpu):
+    # Whatever bits the caller passes, the count is the reference recursion's.
+    rng = np.random.default_rng(11)
+    for N in (1, 2, 5, 8, 10, 12):
+        n = 4000
+        cols = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+        cols &= rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+        cols &= rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+        keep = rng.random(n) < 0.7
+        cols[keep] &= np.uint32((1 << N) - 1)
+        ld = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32) & rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+        rd = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32) & rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+        want = oracle.count_tasks(N, cols, ld, rd)
+        res = gpu.count_tasks(N, cols, ld, rd, per_task=True)
+        assert np.array_equal(res["per_task"], want), N
+
+
+def test_edge_tasks(gpu):
+    N = 8
+    last = (1 << N) - 1
+    cols = np.array([last, last | 256, 0, 0b1, 0xFF00, 0], np.uint32)
+    ld = np.array([0, 0, 0, 0, 0, 0xFF], np.uint32)
+    rd = np.array([0, 0, 0, 0, 0, 0], np.uint32)
+    want = oracle.count_tasks(N, cols, ld, rd)
+    assert list(want) == [1, 0, 92, oracle.count_task(8, 1, 0, 0), 0, 0]
+    res = gpu.count_tasks(N, cols, ld, rd, per_task=True)
+    assert np.array_equal(res["per_task"], want)
+    empty = gpu.count_tasks(N, [], [], [], per_task=True)
+    assert empty["sum"] == 0 and empty["per_task"].size == 0
+
+
+def test_launch_shapes_and_order_give_same_count(gpu, golden):
+    pub = golden("published.json")
+    N, k = 17, 6
+    c, l, r = oracle.expand(N, k)
+    want = pub[str(N)]["total"]
+    for cfg in [dict(block_threads=64), dict(block_threads=128, blocks_per_sm=1), dict(block_threads=512),
+                dict(steal=-1), dict(inner_steps=4), dict(inner_steps=1024), dict(stack_levels=20)]:
+        assert 2 * gpu.count_tasks(N, c, l, r, config=cfg)["sum"] == want, cfg
+    perm = np.random.default_rng(2).permutation(c.size).astype(np.uint32)
+    cfg = gpu.Config()
+    cfg.order_kind = gpu.NQ_ORDER_GIVEN
+    cfg.order = perm.ctypes.data
+    res = gpu.count_tasks(N, c, l, r, per_task=True, config=cfg)
+    assert 2 * res["sum"] == want
+    assert np.array_equal(res["per_task"], oracle.count_tasks(N, c, l, r))
+
+
+def test_depth_error_is_reported(gpu):
+    with pytest.raises(gpu.NQError) as e:
+        gpu.count(16, 5, config=dict(stack_levels=3))
+    assert e.value.status == gpu.NQ_ERR_DEPTH
+    # The context stays usable.
+    assert gpu.count(12, 4).total == 14200
+
+
+def test_time_limit_stops_kernel_and_context_survives(gpu, golden):
+    with pytest.raises(gpu.NQError) as e:
+        gpu.count(19, 6, config=dict(time_limit_ms=1))
+    assert e.value.status == gpu.NQ_ERR_TIMEOUT
+    assert gpu.count(13, 5).total == golden("published.json")["13"]["total"]
+
+
+def test_device_entry_with_torch_tensors(gpu, golden):
+    import torch
+    N, k = 16, 5
+    c, l, r = oracle.expand(N, k)
+    dev = torch.device("cuda:0")
+    tc = torch.from_numpy(c.view(np.int32)).to(dev)
+    tl = torch.from_numpy(l.view(np.int32)).to(dev)
+    tr = torch.from_numpy(r.view(np.int32)).to(dev)
+    out = torch.zeros(2, dtype=torch.int64, device=dev)
+    per = torch.zeros(c.size, dtype=torch.int64, device=dev)
+    gpu.count_tasks_device(N, tc, tl, tr, out, per_task=per, config=dict(stack_levels=N - 1 - k),
+                           stream=torch.cuda.current_stream())
+    torch.cuda.synchronize()
+    assert 2 * int(out[0]) == golden("published.json")[str(N)]["total"]
+    assert int(out[1]) == 0
+    assert np.array_equal(per.cpu().numpy().view(np.uint64), oracle.count_tasks(N, c, l, r))
+    # Too few stack levels: the status word says so.
+    gpu.count_tasks_device(N, tc, tl, tr, out, config=dict(stack_levels=2), stream=torch.cuda.current_stream())
+    torch.cuda.synchronize()
+    assert int(out[1]) & 1
+
+
+def test_batch_small_boards(gpu, golden):
+    g = golden("boards_small.json")
+    inst = [tuple(b) for b in g["instances"]]
+    for split in (0, 1, 3, 5):
+        out = gpu.count_batch(inst, split_rows=split)
+        assert out.tolist() == g["counts"], split
+
+
+def test_dropin_n_queens_single_board(gpu):
+    for (N, c, l, r) in workloads.random_boards(20, 9, 8, 15, 0, 4):
+        assert gpu.n_queens(N, c, l, r) == oracle.count_task(N, c, l, r)
+
+
+def test_cli_result_line(gpu):
+    import subprocess
+    out = subprocess.run([gpu.CLI_PATH, "16", "5"], capture_output=True, text=True, timeout=300).stdout
+    assert "cuda 16 queens result 14772512, calc time: [" in out
+    assert "to generate 70906 subproblems!" in out
+    assert "gpu [0] start job, with 70906(1.00) subproblems." in out
