@@ -48,9 +48,11 @@ METRIC = "DFS nodes/s (exact whole-board count, 1 B200)"
 # statistics and, up to N=17, by the CPU oracle).
 WORKLOADS = {
     "n16k5": dict(N=16, k=5, total=14772512, nodes=563126914),
+    "n17k6": dict(N=17, k=6, total=95815104, nodes=3959755915),
+    "n18k6": dict(N=18, k=6, total=666090624, nodes=29348496950),
     "n19k6": dict(N=19, k=6, total=4968057848, nodes=228483606026),
     "n20k6": dict(N=20, k=6, total=39029188884, nodes=1865470950135),
-    "n21k6": dict(N=21, k=6, total=314666222712, nodes=None),
+    "n21k6": dict(N=21, k=6, total=314666222712, nodes=15916200586353),
     "n22k6": dict(N=22, k=6, total=2691008701644, nodes=None),
 }
 

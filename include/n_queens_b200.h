@@ -116,7 +116,10 @@ int nq_expand(int N, int rows, uint32_t *cols, uint32_t *ld, uint32_t *rd, int64
  * per-prefix counts in *total (the reference's x2 mirror reduction,
  * src/n_queens_cuda.cu:181-183).  Requires 2 <= N <= NQ_MAX_N and
  * 1 <= rows <= N-2 (src/main.cpp:21-24).  If nodes is not NULL the DFS
- * node total of the same decomposition is counted as well (slower). */
+ * node total of the same decomposition is counted as well (slower).
+ * As in the reference, odd N with rows == 1 overcounts (the middle-column
+ * task is doubled without the second-row restriction); the reference CLI
+ * raises rows to 2 (src/main.cpp:26-29) and so does this library's CLI. */
 int nq_count(int N, int rows, const nq_config *cfg, uint64_t *total, uint64_t *nodes, nq_stats *stats);
 
 /* Counts over a caller-built task list in host memory.  Replaces the
@@ -131,9 +134,13 @@ int nq_count_tasks(int N, const uint32_t *cols, const uint32_t *ld, const uint32
 
 /* The same over device-resident tasks (device pointers, already in HBM),
  * enqueued on `stream` (a cudaStream_t; NULL = legacy default stream).
- * d_per_task / d_nodes are optional device arrays of n uint64 (overwritten);
- * d_sum is a device uint64 (overwritten).  Returns after enqueueing; the
- * caller synchronises the stream.  Uses the library's device scratch for the
+ * d_per_task / d_nodes are optional device arrays of n uint64 (overwritten;
+ * d_nodes needs d_per_task).  d_sum is a device array of 2 uint64: [0]
+ * receives the plain sum of the counts, [1] status bits (1: a task needed
+ * more stack levels than the launch had and was skipped; 2: the time limit
+ * stopped the kernel).  Without a host view of the tasks the stack covers
+ * N-1 levels unless cfg->stack_levels says less.  Returns after enqueueing;
+ * the caller synchronises the stream.  Uses the library's device scratch for the
  * queue and the per-CTA partials, so calls on one device must not overlap. */
 int nq_count_tasks_device(int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd, int64_t n,
                           uint64_t *d_per_task, uint64_t *d_nodes, uint64_t *d_sum, const nq_config *cfg,

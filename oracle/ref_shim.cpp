@@ -47,7 +47,7 @@ long long nqref_parallel(int N, int rows) { return parallel_n_queens(N, rows); }
 long long nqref_count_tasks(int N, long long n, const int *tot, long long *out, int threads) {
     vector<long long> partial(n > 0 ? n : 1, 0);
     if (threads <= 0) threads = omp_get_max_threads();
-#pragma omp parallel for schedule(dynamic, 16) num_threads(threads)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
     for (long long i = 0; i < n; i++) {
         n_queens(N, tot[3 * i], tot[3 * i + 1], tot[3 * i + 2], partial[i]);
     }

@@ -34,8 +34,8 @@ from n_queens_b200 import workloads  # noqa: E402
 EXPANDER_CASES = [(2, 1), (4, 1), (4, 2), (5, 1), (5, 2), (5, 3), (6, 2), (6, 4), (7, 3), (7, 5), (8, 1), (8, 2),
                   (8, 6), (9, 2), (9, 3), (9, 7), (10, 4), (11, 4), (11, 5), (12, 4), (13, 5), (14, 5), (15, 5),
                   (16, 5), (16, 6), (17, 6), (18, 6), (19, 6), (20, 6), (21, 6)]
-TOTAL_CASES = [(4, 2), (5, 2), (5, 3), (6, 2), (6, 4), (7, 3), (8, 2), (8, 3), (8, 6), (9, 3), (9, 7), (10, 4),
-               (11, 4), (12, 4), (12, 5), (13, 5), (14, 5), (15, 5), (16, 5)]
+TOTAL_CASES = [(5, 1), (7, 1), (9, 1), (11, 1), (4, 2), (5, 2), (5, 3), (6, 2), (6, 4), (7, 3), (8, 2), (8, 3),
+               (8, 6), (9, 3), (9, 7), (10, 4), (11, 4), (12, 4), (12, 5), (13, 5), (14, 5), (15, 5), (16, 5)]
 PER_TASK_CASES = [(8, 2), (9, 3), (10, 4), (11, 5), (12, 4), (13, 5), (14, 4), (15, 5), (16, 5), (17, 6)]
 
 
@@ -69,14 +69,41 @@ def gen_per_task():
     return out
 
 
+def children(N: int, board, depth: int):
+    """The boards n_queens() recurses into `depth` rows below `board`.
+
+    One recursion step of src/n_queens.cpp:14-19: every free column p of the
+    next row gives (cur|p, (left|p)<<1, (right|p)>>1).  n_queens() of a board
+    is the sum of n_queens() over these children unless the board is already
+    complete, so splitting here only spreads the reference's own recursion
+    over more OpenMP iterations.
+    """
+    last = (1 << N) - 1
+    out = [board]
+    for _ in range(depth):
+        nxt = []
+        for (c, l, r) in out:
+            if c == last:
+                nxt.append((c, l, r))
+                continue
+            v = last & ~(c | l | r)
+            while v:
+                p = v & -v
+                v ^= p
+                nxt.append((c | p, ((l | p) << 1) & 0xFFFFFFFF, (r | p) >> 1))
+        out = nxt
+    return out
+
+
 def gen_boards(n: int, seed: int, n_lo: int, n_hi: int, m_lo: int, m_hi: int, threads: int = 0):
     """Reference counts of a seeded batch of partial boards.
 
     Identical boards are counted once, and a board and its mirror image
     (workloads.mirror_board, same count) share one count.  Empty boards of
     N >= 17 take their totals from the reference's README (their recursion
-    would take hours); all other boards run through the reference's
-    n_queens().
+    would take hours).  All other boards run through the reference's
+    n_queens(); boards with N >= 17 and few queens are first split into
+    their recursion children (see children()) so the OpenMP loop balances.
     """
     published = {int(k): v["total"] for k, v in json.load(open(os.path.join(HERE, "published.json"))).items()}
     boards = workloads.random_boards(n, seed, n_lo, n_hi, m_lo, m_hi)
@@ -100,11 +127,20 @@ def gen_boards(n: int, seed: int, n_lo: int, n_hi: int, m_lo: int, m_hi: int, th
         byN.setdefault(b[0], []).append(b)
     for N in sorted(byN):
         lst = byN[N]
-        aos = np.array([[b[1], b[2], b[3]] for b in lst], dtype=np.uint32).view(np.int32)
+        pieces, owner = [], []
+        for i, b in enumerate(lst):
+            m = bin(b[1]).count("1")
+            depth = max(0, min(3, N - 16 - m)) if N >= 17 else 0
+            for ch in children(N, b[1:], depth):
+                pieces.append(ch)
+                owner.append(i)
+        aos = np.array(pieces, dtype=np.uint32).reshape(-1, 3).view(np.int32)
         t = time.time()
         _, per = oracle.ref_count_tasks(N, aos, threads=threads, per_task=True)
-        print(f"  N={N}: {len(lst)} distinct boards in {time.time() - t:.1f}s", flush=True)
-        for b, v in zip(lst, per.tolist()):
+        sums = np.zeros(len(lst), np.int64)
+        np.add.at(sums, np.array(owner), per)
+        print(f"  N={N}: {len(lst)} distinct boards ({len(pieces)} pieces) in {time.time() - t:.1f}s", flush=True)
+        for b, v in zip(lst, sums.tolist()):
             counts[b] = int(v)
     return {"seed": seed, "n": n, "N_range": [n_lo, n_hi], "m_range": [m_lo, m_hi],
             "instances": [[b[0], b[1], b[2], b[3]] for b in boards],
