@@ -12,6 +12,7 @@
 //  * errors come back as nq_status codes; the library never exits.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -60,9 +61,32 @@ double now_ms() {
 
 typedef void (*KernelFn)(DfsParams);
 
-KernelFn pick_kernel(bool per_owner, bool nodes) {
-    if (per_owner) return nodes ? dfs_kernel<true, true> : dfs_kernel<true, false>;
-    return nodes ? dfs_kernel<false, true> : dfs_kernel<false, false>;
+// Step variant (see dfs_step): 0 = logic ops, unroll 4; 1 = pipe-balanced,
+// unroll 4; 2 = pipe-balanced, unroll 8.
+int g_variant = -1;
+
+int step_variant() {
+    if (g_variant < 0) {
+        const char *v = getenv("NQB_VARIANT");
+        g_variant = v ? atoi(v) : 2;
+        if (g_variant < 0 || g_variant > 2) g_variant = 2;
+    }
+    return g_variant;
+}
+
+template <bool PO, bool ND>
+KernelFn pick_variant(int v) {
+    switch (v) {
+        case 0: return dfs_kernel<PO, ND, 0, 4>;
+        case 1: return dfs_kernel<PO, ND, 1, 4>;
+        default: return dfs_kernel<PO, ND, 1, 8>;
+    }
+}
+
+KernelFn pick_kernel(bool per_owner, bool nodes, int v = -1) {
+    if (v < 0) v = step_variant();
+    if (per_owner) return nodes ? pick_variant<true, true>(v) : pick_variant<true, false>(v);
+    return nodes ? pick_variant<false, true>(v) : pick_variant<false, false>(v);
 }
 
 struct DevBuf {
@@ -138,8 +162,9 @@ int ensure_ready(Ctx &c, int dev) {
     const int static_smem = 2 * 32 * 8 + 16;
     for (int po = 0; po < 2; ++po)
         for (int nd = 0; nd < 2; ++nd)
-            NQ_CUDA(cudaFuncSetAttribute(pick_kernel(po, nd), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         c.smem_optin - static_smem));
+            for (int v = 0; v < 3; ++v)
+                NQ_CUDA(cudaFuncSetAttribute(pick_kernel(po, nd, v), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             c.smem_optin - static_smem));
     c.ready = true;
     return NQ_OK;
 }
@@ -233,6 +258,9 @@ DfsParams base_params(Ctx &c, int N, int64_t n, const nq_config *cfg) {
     p.nodes_out = c.d_ctl + kWordNodes;
     p.status_out = c.d_ctl + kWordStatus;
     p.block_cnt = c.d_ctl + kWordBlocks;
+    p.k_one = 1;
+    p.k_two = 2;
+    p.k_mone = 0xffffffffu;
     p.block_nodes = c.d_ctl + kWordBlocks + (size_t)c.sms * kMaxBlocksPerSm;
     return p;
 }

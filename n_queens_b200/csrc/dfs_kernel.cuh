@@ -74,6 +74,7 @@ struct DfsParams {
     unsigned long long *sum_out;     // total count (device word)
     unsigned long long *nodes_out;   // total nodes (device word, NODES)
     unsigned long long *status_out;  // kStat* bits of this launch (device word)
+    uint32_t k_one, k_two, k_mone;   // 1, 2, -1 (see dfs_step)
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -102,43 +103,24 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
 //   otherwise, level exhausted  -> pop a stacked level if there is one
 // An idle lane (avail == 0, empty stack) passes through with no effect.
 // Right shift is arithmetic, as in the reference's `int` arithmetic.
-#define NQB_STEP_ASM                                                                  \
+//
+// Operands: %0 cols, %1 ld, %2 rd, %3 avail, %4 sp, %5 cnt, %6 placements
+// (node statistics), %7 bot, %8 = 1, %9 = 2, %10 = -1.  The three constants
+// arrive as kernel parameters, so the compiler cannot fold the multiply-adds
+// below back into ALU adds/moves.
+//
+// VAR 0 issues everything as logic/ALU operations.  VAR 1 moves the adds,
+// the left shift and the four register moves to multiply-add form (the FMA
+// pipe), leaving the LOP3/shift/compare work on the ALU pipe: about 11
+// instructions on each pipe per step instead of ~17 ALU + 7 FMA.
+#define NQB_STEP_HEAD                                                                 \
     "{\n\t"                                                                           \
     ".reg .pred pb, pd, pp, pe, pq;\n\t"                                              \
-    ".reg .b32 bit, nc, nl, nr, na;\n\t"                                              \
-    "neg.s32 bit, %3;\n\t"                                                            \
-    "and.b32 bit, bit, %3;\n\t"                                                       \
-    "xor.b32 %3, %3, bit;\n\t"                                                        \
-    "or.b32 nc, %0, bit;\n\t"                                                         \
-    "or.b32 nl, %1, bit;\n\t"                                                         \
-    "shl.b32 nl, nl, 1;\n\t"                                                          \
-    "or.b32 nr, %2, bit;\n\t"                                                         \
-    "shr.s32 nr, nr, 1;\n\t"                                                          \
-    "lop3.b32 na, nc, nl, nr, 0x01;\n\t"                                              \
-    "setp.eq.u32 pe, nc, 0xffffffff;\n\t"                                             \
-    "@pe add.u32 %5, %5, 1;\n\t"                                                      \
-    "setp.ne.u32 pb, bit, 0;\n\t"                                                     \
-    "setp.ne.and.u32 pd, na, 0, pb;\n\t"                                              \
-    "setp.ne.and.u32 pp, %3, 0, pd;\n\t"                                              \
-    "@pp st.shared.v4.u32 [%4], {%0, %1, %2, %3};\n\t"                                \
-    "@pp add.u32 %4, %4, 512;\n\t"                                                    \
-    "@pd mov.b32 %0, nc;\n\t"                                                         \
-    "@pd mov.b32 %1, nl;\n\t"                                                         \
-    "@pd mov.b32 %2, nr;\n\t"                                                         \
-    "@pd mov.b32 %3, na;\n\t"                                                         \
-    "setp.eq.u32 pq, %3, 0;\n\t"                                                      \
-    "setp.ne.and.u32 pq, %4, %6, pq;\n\t"                                             \
-    "@pq sub.u32 %4, %4, 512;\n\t"                                                    \
-    "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"                                \
-    "}\n\t"
+    ".reg .b32 t, bit, nc, nl, nr, na;\n\t"
 
-// Same step, also counting placements (for the node statistics).
-#define NQB_STEP_ASM_NODES                                                            \
-    "{\n\t"                                                                           \
-    ".reg .pred pb, pd, pp, pe, pq;\n\t"                                              \
-    ".reg .b32 bit, nc, nl, nr, na;\n\t"                                              \
-    "neg.s32 bit, %3;\n\t"                                                            \
-    "and.b32 bit, bit, %3;\n\t"                                                       \
+#define NQB_STEP_CHILD_VAR0                                                           \
+    "neg.s32 t, %3;\n\t"                                                              \
+    "and.b32 bit, t, %3;\n\t"                                                         \
     "xor.b32 %3, %3, bit;\n\t"                                                        \
     "or.b32 nc, %0, bit;\n\t"                                                         \
     "or.b32 nl, %1, bit;\n\t"                                                         \
@@ -148,8 +130,26 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "lop3.b32 na, nc, nl, nr, 0x01;\n\t"                                              \
     "setp.eq.u32 pe, nc, 0xffffffff;\n\t"                                             \
     "@pe add.u32 %5, %5, 1;\n\t"                                                      \
+    "setp.ne.u32 pb, bit, 0;\n\t"
+
+#define NQB_STEP_CHILD_VAR1                                                           \
+    "mul.lo.s32 t, %3, %10;\n\t"                                                      \
+    "and.b32 bit, t, %3;\n\t"                                                         \
     "setp.ne.u32 pb, bit, 0;\n\t"                                                     \
-    "@pb add.u32 %6, %6, 1;\n\t"                                                      \
+    "mad.lo.s32 %3, bit, %10, %3;\n\t"                                                \
+    "mad.lo.s32 nc, bit, %8, %0;\n\t"                                                 \
+    "or.b32 nl, %1, bit;\n\t"                                                         \
+    "mul.lo.s32 nl, nl, %9;\n\t"                                                      \
+    "or.b32 nr, %2, bit;\n\t"                                                         \
+    "shr.s32 nr, nr, 1;\n\t"                                                          \
+    "lop3.b32 na, nc, nl, nr, 0x01;\n\t"                                              \
+    "setp.eq.u32 pe, nc, 0xffffffff;\n\t"                                             \
+    "@pe mad.lo.s32 %5, %8, %8, %5;\n\t"
+
+#define NQB_STEP_NODES_VAR0 "@pb add.u32 %6, %6, 1;\n\t"
+#define NQB_STEP_NODES_VAR1 "@pb mad.lo.s32 %6, %8, %8, %6;\n\t"
+
+#define NQB_STEP_TAIL_VAR0                                                            \
     "setp.ne.and.u32 pd, na, 0, pb;\n\t"                                              \
     "setp.ne.and.u32 pp, %3, 0, pd;\n\t"                                              \
     "@pp st.shared.v4.u32 [%4], {%0, %1, %2, %3};\n\t"                                \
@@ -164,30 +164,45 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"                                \
     "}\n\t"
 
-template <bool NODES>
-struct Step;
+#define NQB_STEP_TAIL_VAR1                                                            \
+    "setp.ne.and.u32 pd, na, 0, pb;\n\t"                                              \
+    "setp.ne.and.u32 pp, %3, 0, pd;\n\t"                                              \
+    "@pp st.shared.v4.u32 [%4], {%0, %1, %2, %3};\n\t"                                \
+    "@pp mad.lo.s32 %4, %8, 512, %4;\n\t"                                             \
+    "@pd mul.lo.s32 %0, nc, %8;\n\t"                                                  \
+    "@pd mul.lo.s32 %1, nl, %8;\n\t"                                                  \
+    "@pd mul.lo.s32 %2, nr, %8;\n\t"                                                  \
+    "@pd mul.lo.s32 %3, na, %8;\n\t"                                                  \
+    "setp.eq.u32 pq, %3, 0;\n\t"                                                      \
+    "setp.ne.and.u32 pq, %4, %7, pq;\n\t"                                             \
+    "@pq mad.lo.s32 %4, %8, -512, %4;\n\t"                                            \
+    "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"                                \
+    "}\n\t"
 
-template <>
-struct Step<false> {
-    static __device__ __forceinline__ void run(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail,
-                                               uint32_t &sp, uint32_t &cnt, uint32_t bot, uint32_t &) {
-        asm volatile(NQB_STEP_ASM
-                     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt)
-                     : "r"(bot)
-                     : "memory");
-    }
+struct StepConsts {
+    uint32_t one, two, mone;
 };
 
-template <>
-struct Step<true> {
-    static __device__ __forceinline__ void run(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail,
-                                               uint32_t &sp, uint32_t &cnt, uint32_t bot, uint32_t &it) {
-        asm volatile(NQB_STEP_ASM_NODES
-                     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
-                     : "r"(bot)
-                     : "memory");
+template <bool NODES, int VAR>
+__device__ __forceinline__ void dfs_step(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail, uint32_t &sp,
+                                         uint32_t &cnt, uint32_t &it, uint32_t bot, const StepConsts &k) {
+#define NQB_STEP_OPERANDS                                                                         \
+    : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)                   \
+    : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone)                                               \
+    : "memory"
+    if (VAR == 0) {
+        if (NODES)
+            asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR0 NQB_STEP_NODES_VAR0 NQB_STEP_TAIL_VAR0 NQB_STEP_OPERANDS);
+        else
+            asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR0 NQB_STEP_TAIL_VAR0 NQB_STEP_OPERANDS);
+    } else {
+        if (NODES)
+            asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR1 NQB_STEP_NODES_VAR1 NQB_STEP_TAIL_VAR1 NQB_STEP_OPERANDS);
+        else
+            asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR1 NQB_STEP_TAIL_VAR1 NQB_STEP_OPERANDS);
     }
-};
+#undef NQB_STEP_OPERANDS
+}
 
 // Loads task t into a lane.  Returns the completions credited immediately
 // (1 for an already-complete board) and leaves avail == 0 when the task has
@@ -217,7 +232,7 @@ __device__ __forceinline__ uint32_t load_task(const DfsParams &p, long long t, u
     return 0;
 }
 
-template <bool PER_OWNER, bool NODES>
+template <bool PER_OWNER, bool NODES, int VAR, int UNROLL>
 __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long red_cnt[32];
@@ -229,6 +244,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
     const uint32_t smem_base = (uint32_t)__cvta_generic_to_shared(smem_raw);
     const uint32_t my_base = smem_base + warp * (uint32_t)p.levels * kSlotBytes + lane * 16u;
 
+    const StepConsts kc{p.k_one, p.k_two, p.k_mone};
     uint32_t cols = 0, ld = 0, rd = 0, avail = 0;
     uint32_t sp = my_base, bot = my_base;
     uint32_t cnt = 0, it = 0;
@@ -346,19 +362,15 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
 
         // ---- DFS steps
         if (check_idle) {
-            for (int s = 0; s < p.inner; s += 4) {
-                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
-                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
-                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
-                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
+            for (int s = 0; s < p.inner; s += UNROLL) {
+#pragma unroll
+                for (int u = 0; u < UNROLL; ++u) dfs_step<NODES, VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
                 if (__any_sync(kFull, avail == 0)) break;
             }
         } else {
-            for (int s = 0; s < p.inner; s += 4) {
-                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
-                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
-                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
-                Step<NODES>::run(cols, ld, rd, avail, sp, cnt, bot, it);
+            for (int s = 0; s < p.inner; s += UNROLL) {
+#pragma unroll
+                for (int u = 0; u < UNROLL; ++u) dfs_step<NODES, VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
                 if (__all_sync(kFull, avail == 0)) break;
             }
         }
