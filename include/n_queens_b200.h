@@ -146,6 +146,23 @@ int nq_count_tasks_device(int N, const uint32_t *d_cols, const uint32_t *d_ld, c
                           uint64_t *d_per_task, uint64_t *d_nodes, uint64_t *d_sum, const nq_config *cfg,
                           void *stream);
 
+/* Device-resident count that allocates nothing.  No counterpart in the
+ * reference: it exists for callers that cannot let a library call cudaMalloc
+ * -- a host framework whose caching allocator has reserved the GPU's memory,
+ * or a service that forbids device allocation after start-up.  Same inputs,
+ * outputs and meaning as nq_count_tasks_device without per-task outputs:
+ * d_sum (2 device uint64) receives the plain sum and the status bits.  The
+ * queue/flag words and per-CTA partials live in a fixed array inside the
+ * library image (about 64 KiB, held on every GPU that loads the library until
+ * exit) with room for 8192 CTAs; a cfg->blocks_per_sm that would launch more
+ * is rejected with NQ_ERR_ARG.  Every call shares that array and clears its
+ * control words first, so calls whose kernels overlap on the GPU race and
+ * must be serialised by the caller.  The first call on a device performs the
+ * device's set-up (the array's device address, the kernel's shared-memory
+ * opt-in); make it before any stream capture. */
+int nq_count_tasks_device_noalloc(int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd,
+                                  int64_t n, uint64_t *d_sum, const nq_config *cfg, void *stream);
+
 /* Batched independent instances of uneven N and partial boards in one
  * persistent launch.  Each instance is split into subtasks at split_rows
  * extra rows (0 = autotuned) and out[i] receives its completions (no

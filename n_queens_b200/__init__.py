@@ -126,6 +126,9 @@ def _load() -> ctypes.CDLL:
     L.nq_count_tasks_device.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                         ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _cfgp,
                                         ctypes.c_void_p]
+    L.nq_count_tasks_device_noalloc.restype = ctypes.c_int
+    L.nq_count_tasks_device_noalloc.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_int64, ctypes.c_void_p, _cfgp, ctypes.c_void_p]
     L.nq_count_batch.restype = ctypes.c_int
     L.nq_count_batch.argtypes = [ctypes.POINTER(Instance), ctypes.c_int64, ctypes.c_int, _u64p, _cfgp, _stp]
     return L
@@ -135,7 +138,7 @@ lib = _load()
 
 # Every symbol the C header declares (checked by the CPU test suite).
 EXPORTS = ("nq_abi_version", "nq_status_string", "nq_last_error", "nq_device_count", "nq_expand", "nq_count",
-           "nq_count_tasks", "nq_count_tasks_device", "nq_count_batch")
+           "nq_count_tasks", "nq_count_tasks_device", "nq_count_tasks_device_noalloc", "nq_count_batch")
 
 
 def status_string(status: int) -> str:

@@ -364,6 +364,8 @@ int count_resident(Ctx &c, int N, const uint32_t *d_cols, const uint32_t *d_ld, 
 
 }  // namespace
 
+void set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+
 }  // namespace nqb
 
 using namespace nqb;
