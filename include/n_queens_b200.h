@@ -66,7 +66,9 @@ typedef struct nq_config {
                                pointer, matching the entry's other task arrays) */
     uint32_t time_limit_ms; /* 0 = none; else the kernel stops after this long (NQ_ERR_TIMEOUT) */
     int device;             /* CUDA device ordinal (default 0) */
-    int reserved[6];
+    int timing;             /* non-zero: host entries record per-CTA start/end times and fill the
+                               makespan / tail fields of nq_stats */
+    int reserved[5];
 } nq_config;
 
 /* Timings and sizes of one call (all optional outputs). */
@@ -83,6 +85,14 @@ typedef struct nq_stats {
     int stack_levels;   /* stack slots per lane */
     int smem_bytes;     /* dynamic shared memory per CTA */
     int reserved[5];
+    /* With nq_config.timing: kernel span from the first CTA start to the last
+     * CTA end, the mean CTA busy time, and the idle fraction of the grid
+     * (1 - sum of CTA busy times / (CTAs x span)) -- the tail left by uneven
+     * tasks. */
+    double makespan_ms;
+    double cta_busy_mean_ms;
+    double tail_idle_frac;
+    double schedule_ms; /* nq_count_learned: prediction + longest-first sort */
 } nq_stats;
 
 /* One independent completion-counting problem of the batched entry. */
@@ -169,6 +179,52 @@ int nq_count_tasks_device_noalloc(int N, const uint32_t *d_cols, const uint32_t 
  * symmetry factor, as n_queens() counts them). */
 int nq_count_batch(const nq_instance *inst, int64_t n, int split_rows, uint64_t *out, const nq_config *cfg,
                    nq_stats *stats);
+
+/* ---- Learned subtree-cost scheduler (no counterpart in the reference) ----
+ *
+ * The reference hands tasks out in expander order (src/n_queens_cuda.cu:10,80).
+ * These entries build and use a small cost model so the queue can run the
+ * most expensive prefixes first.  Model: the three masks of a task as 96 bits
+ * (cols, ld, rd, 32 bits each, columns >= N cleared) -> 128 ReLU -> 128 ReLU
+ * -> predicted log2(1 + DFS nodes).  BF16 weights for compute, FP32 master
+ * weights and Adam, FP32 accumulation; every kernel is this library's own.
+ * A model lives on one device; calls on one model are serialised. */
+typedef struct nq_mlp nq_mlp;
+
+/* Number of FP32 parameters (29057).  Flat layout: W1[128][96], b1[128],
+ * W2[128][128], b2[128], W3[128], b3. */
+int nq_mlp_num_params(void);
+/* New model on `device`, weights ~ U(-1/sqrt(fan_in), 1/sqrt(fan_in)) from
+ * SplitMix64(seed). */
+int nq_mlp_create(int device, uint64_t seed, nq_mlp **out);
+int nq_mlp_destroy(nq_mlp *m);
+/* FP32 master weights in the flat layout; set also resets Adam's moments. */
+int nq_mlp_get_params(nq_mlp *m, float *out);
+int nq_mlp_set_params(nq_mlp *m, const float *in);
+/* Predicted log2(1 + nodes) of n tasks of board size N (host arrays). */
+int nq_mlp_predict(nq_mlp *m, int N, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd, int64_t n,
+                   float *out);
+/* Gradient of the mean squared error over n tasks (per-task board sizes in
+ * task_n, targets in log2(1 + nodes)) with respect to the BF16 compute
+ * weights, in the flat layout, and the loss.  Changes nothing. */
+int nq_mlp_grad(nq_mlp *m, const uint8_t *task_n, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd,
+                const float *target, int64_t n, float *grad_out, float *loss_out);
+/* Adam (beta 0.9/0.999, eps 1e-8) over `epochs` shuffled passes (SplitMix64
+ * seed) in minibatches of `batch`; epoch_loss (optional, `epochs` floats)
+ * receives each pass's mean squared error. */
+int nq_mlp_train(nq_mlp *m, const uint8_t *task_n, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd,
+                 const float *target, int64_t n, int epochs, int batch, float lr, uint64_t seed,
+                 float *epoch_loss);
+/* Longest-first order of device-resident tasks: d_order (n u32) receives the
+ * task indices sorted by predicted cost, descending, in bins of 1/8 log2 unit
+ * and stable inside a bin; d_pred (optional, n floats) the predictions.
+ * Stream-ordered on `stream`. */
+int nq_schedule_device(nq_mlp *m, int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd,
+                       int64_t n, uint32_t *d_order, float *d_pred, void *stream);
+/* nq_count with the queue ordered by the model: expand, upload, schedule on
+ * the device, count.  The same total as nq_count; stats->schedule_ms holds the
+ * prediction + sort time.  The model must live on cfg->device. */
+int nq_count_learned(int N, int rows, nq_mlp *m, const nq_config *cfg, uint64_t *total, nq_stats *stats);
 
 #ifdef __cplusplus
 }

@@ -15,7 +15,8 @@ Reference interface this mirrors (ygch/n_queens, ``src/n_queens.h``):
   here counted on the GPU.
 
 and adds the library's own entries: :func:`count`, :func:`count_tasks`,
-:func:`count_tasks_device`, :func:`count_batch`.
+:func:`count_tasks_device`, :func:`count_batch`, and (``n_queens_b200.learned``)
+the learned subtree-cost scheduler.
 """
 from __future__ import annotations
 
@@ -64,7 +65,8 @@ class Config(ctypes.Structure):
         ("order", ctypes.c_void_p),
         ("time_limit_ms", ctypes.c_uint32),
         ("device", ctypes.c_int),
-        ("reserved", ctypes.c_int * 6),
+        ("timing", ctypes.c_int),
+        ("reserved", ctypes.c_int * 5),
     ]
 
 
@@ -84,6 +86,10 @@ class Stats(ctypes.Structure):
         ("stack_levels", ctypes.c_int),
         ("smem_bytes", ctypes.c_int),
         ("reserved", ctypes.c_int * 5),
+        ("makespan_ms", ctypes.c_double),
+        ("cta_busy_mean_ms", ctypes.c_double),
+        ("tail_idle_frac", ctypes.c_double),
+        ("schedule_ms", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -138,7 +144,9 @@ lib = _load()
 
 # Every symbol the C header declares (checked by the CPU test suite).
 EXPORTS = ("nq_abi_version", "nq_status_string", "nq_last_error", "nq_device_count", "nq_expand", "nq_count",
-           "nq_count_tasks", "nq_count_tasks_device", "nq_count_tasks_device_noalloc", "nq_count_batch")
+           "nq_count_tasks", "nq_count_tasks_device", "nq_count_tasks_device_noalloc", "nq_count_batch",
+           "nq_mlp_num_params", "nq_mlp_create", "nq_mlp_destroy", "nq_mlp_get_params", "nq_mlp_set_params",
+           "nq_mlp_predict", "nq_mlp_grad", "nq_mlp_train", "nq_schedule_device", "nq_count_learned")
 
 
 def status_string(status: int) -> str:

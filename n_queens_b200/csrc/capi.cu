@@ -155,7 +155,7 @@ int ensure_ready(Ctx &c, int dev) {
     c.smem_optin = (int)prop.sharedMemPerBlockOptin;
     NQ_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     for (auto &e : c.ev) NQ_CUDA(cudaEventCreate(&e));
-    const size_t ctl_words = kWordBlocks + 2 * (size_t)c.sms * kMaxBlocksPerSm;
+    const size_t ctl_words = kWordBlocks + 4 * (size_t)c.sms * kMaxBlocksPerSm;
     NQ_CUDA(cudaMalloc(&c.d_ctl, ctl_words * sizeof(unsigned long long)));
     NQ_CUDA(cudaMemset(c.d_ctl, 0, ctl_words * sizeof(unsigned long long)));
     // Dynamic shared memory above 48 KiB needs an opt-in per kernel.
@@ -242,6 +242,7 @@ int enqueue_dfs(Ctx &c, DfsParams p, const Launch &L, bool per_owner, bool nodes
     p.inner = L.inner;
     p.steal = L.steal;
     NQ_CUDA(cudaMemsetAsync(p.ctl, 0, kCtlWords * sizeof(unsigned long long), s));
+    if (p.cta_times) NQ_CUDA(cudaMemsetAsync(p.cta_times, 0, 2 * (size_t)L.grid * sizeof(unsigned long long), s));
     pick_kernel(per_owner, nodes)<<<L.grid, L.threads, L.smem, s>>>(p);
     NQ_CUDA(cudaGetLastError());
     return NQ_OK;
@@ -262,6 +263,7 @@ DfsParams base_params(Ctx &c, int N, int64_t n, const nq_config *cfg) {
     p.k_two = 2;
     p.k_mone = 0xffffffffu;
     p.block_nodes = c.d_ctl + kWordBlocks + (size_t)c.sms * kMaxBlocksPerSm;
+    if (cfg && cfg->timing) p.cta_times = c.d_ctl + kWordBlocks + 2 * (size_t)c.sms * kMaxBlocksPerSm;
     return p;
 }
 
@@ -288,11 +290,30 @@ int levels_for_tasks(int N, const uint32_t *cols, int64_t n) {
     return need;
 }
 
+// Per-CTA start/end stamps -> makespan, mean busy time, idle fraction.
+int timing_stats(const unsigned long long *d_times, int grid, nq_stats *st) {
+    std::vector<unsigned long long> t(2 * (size_t)grid);
+    NQ_CUDA(cudaMemcpy(t.data(), d_times, t.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    unsigned long long t0 = ~0ull, t1 = 0;
+    double busy = 0;
+    for (int b = 0; b < grid; ++b) {
+        t0 = std::min(t0, t[2 * b]);
+        t1 = std::max(t1, t[2 * b + 1]);
+        busy += (double)(t[2 * b + 1] - t[2 * b]);
+    }
+    const double span = (double)(t1 - t0);
+    st->makespan_ms = span / 1e6;
+    st->cta_busy_mean_ms = busy / grid / 1e6;
+    st->tail_idle_frac = span > 0 ? 1.0 - busy / (span * grid) : 0.0;
+    return NQ_OK;
+}
+
 // Counts tasks that are already in device memory (d_cols, d_ld, d_rd) and
 // downloads the results.  Used by nq_count and nq_count_tasks.
 int count_resident(Ctx &c, int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd, int64_t n,
                    int levels_needed, const nq_config *cfg, bool per_owner, bool nodes, uint64_t *h_per_task,
-                   uint64_t *h_nodes_task, uint64_t *sum, uint64_t *nodes_total, nq_stats *st, bool timed_h2d) {
+                   uint64_t *h_nodes_task, uint64_t *sum, uint64_t *nodes_total, nq_stats *st, bool timed_h2d,
+                   const uint32_t *d_order = nullptr) {
     Launch L;
     int rc = plan_launch(c, cfg, levels_needed, per_owner, nodes, L);
     if (rc) return rc;
@@ -303,7 +324,7 @@ int count_resident(Ctx &c, int N, const uint32_t *d_cols, const uint32_t *d_ld, 
     p.rd = d_rd;
     // aux layout: [order u32 n] [out_cnt u64 n] [out_nodes u64 n]
     size_t off_order = 0, off_cnt = 0, off_nodes = 0, need = 0;
-    const bool given = cfg && cfg->order_kind == NQ_ORDER_GIVEN && cfg->order;
+    const bool given = !d_order && cfg && cfg->order_kind == NQ_ORDER_GIVEN && cfg->order;
     if (given) {
         off_order = need;
         need += ((size_t)n * 4 + 255) & ~(size_t)255;
@@ -325,6 +346,7 @@ int count_resident(Ctx &c, int N, const uint32_t *d_cols, const uint32_t *d_ld, 
         NQ_CUDA(cudaMemcpyAsync(aux + off_order, cfg->order, (size_t)n * 4, cudaMemcpyHostToDevice, c.stream));
         p.order = (const uint32_t *)(aux + off_order);
     }
+    if (d_order) p.order = d_order;
     if (per_owner) {
         p.out_cnt = (unsigned long long *)(aux + off_cnt);
         NQ_CUDA(cudaMemsetAsync(p.out_cnt, 0, (size_t)n * 8, c.stream));
@@ -345,6 +367,10 @@ int count_resident(Ctx &c, int N, const uint32_t *d_cols, const uint32_t *d_ld, 
         NQ_CUDA(cudaMemcpyAsync(h_nodes_task, p.out_nodes, (size_t)n * 8, cudaMemcpyDeviceToHost, c.stream));
     NQ_CUDA(cudaEventRecord(c.ev[3], c.stream));
     NQ_CUDA(cudaStreamSynchronize(c.stream));
+    if (st && p.cta_times) {
+        rc = timing_stats(p.cta_times, L.grid, st);
+        if (rc) return rc;
+    }
     if (st) {
         float ms = 0;
         if (timed_h2d) {
@@ -476,6 +502,74 @@ int nq_count(int N, int rows, const nq_config *cfg, uint64_t *total, uint64_t *n
     *total = 2 * sum;
     if (nodes) *nodes = nd;
     if (stats) stats->total_ms = now_ms() - t0;
+    return rc;
+}
+
+int nq_count_learned(int N, int rows, nq_mlp *m, const nq_config *cfg, uint64_t *total, nq_stats *stats) {
+    const double t0 = now_ms();
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (N < 2 || N > NQ_MAX_N || rows < 1 || rows > N - 2 || !total || !m) return NQ_ERR_ARG;
+    Ctx *cp = nullptr;
+    int rc = lock_device(device_of(cfg), cp);
+    if (rc) return rc;
+    Ctx &c = *cp;
+    std::lock_guard<std::mutex> lock(c.mu);
+    rc = ensure_ready(c, device_of(cfg));
+    if (rc) return rc;
+    const double te = now_ms();
+    uint32_t *h = nullptr;
+    int grow_rc = NQ_OK;
+    const int64_t n = expand_prefixes_to(
+        N, rows,
+        [&](int64_t total_tasks, uint32_t **pc, uint32_t **pl, uint32_t **pr, int64_t *cap) {
+            grow_rc = c.h_tasks.grow((size_t)std::max<int64_t>(total_tasks, 1) * 12);
+            if (grow_rc) return false;
+            h = (uint32_t *)c.h_tasks.p;
+            *pc = h;
+            *pl = h + total_tasks;
+            *pr = h + 2 * total_tasks;
+            *cap = total_tasks;
+            return true;
+        },
+        0);
+    if (grow_rc) return grow_rc;
+    if (n < 0 || n > 0xffffffffll) return NQ_ERR_ARG;
+    if (stats) {
+        stats->expand_ms = now_ms() - te;
+        stats->tasks = n;
+    }
+    // tasks (12 B each) followed by the order (4 B each)
+    rc = c.tasks.grow((size_t)std::max<int64_t>(n, 1) * 16 + 256);
+    if (rc) return rc;
+    uint32_t *d = (uint32_t *)c.tasks.p;
+    uint32_t *d_order = d + 3 * n;
+    NQ_CUDA(cudaEventRecord(c.ev[0], c.stream));
+    if (n) NQ_CUDA(cudaMemcpyAsync(d, h, (size_t)n * 12, cudaMemcpyHostToDevice, c.stream));
+    cudaEvent_t e_sched0 = nullptr, e_sched1 = nullptr;
+    NQ_CUDA(cudaEventCreate(&e_sched0));
+    NQ_CUDA(cudaEventCreate(&e_sched1));
+    NQ_CUDA(cudaEventRecord(e_sched0, c.stream));
+    rc = nq_schedule_device(m, N, d, d + n, d + 2 * n, n, d_order, nullptr, c.stream);
+    if (rc) {
+        cudaEventDestroy(e_sched0);
+        cudaEventDestroy(e_sched1);
+        return rc;
+    }
+    NQ_CUDA(cudaEventRecord(e_sched1, c.stream));
+    uint64_t sum = 0;
+    rc = count_resident(c, N, d, d + n, d + 2 * n, n, N - 1 - rows, cfg, false, false, nullptr, nullptr, &sum,
+                        nullptr, stats, true, d_order);
+    if (stats) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e_sched0, e_sched1);
+        stats->schedule_ms = ms;
+        cudaEventElapsedTime(&ms, c.ev[0], e_sched0);
+        stats->h2d_ms = ms;
+        stats->total_ms = now_ms() - t0;
+    }
+    cudaEventDestroy(e_sched0);
+    cudaEventDestroy(e_sched1);
+    *total = 2 * sum;
     return rc;
 }
 

@@ -75,6 +75,7 @@ struct DfsParams {
     unsigned long long *nodes_out;   // total nodes (device word, NODES)
     unsigned long long *status_out;  // kStat* bits of this launch (device word)
     uint32_t k_one, k_two, k_mone;   // 1, 2, -1 (see dfs_step)
+    unsigned long long *cta_times;   // optional [2*gridDim.x]: %globaltimer at CTA start and end
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -244,6 +245,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
     const uint32_t smem_base = (uint32_t)__cvta_generic_to_shared(smem_raw);
     const uint32_t my_base = smem_base + warp * (uint32_t)p.levels * kSlotBytes + lane * 16u;
 
+    if (p.cta_times && threadIdx.x == 0) p.cta_times[2 * blockIdx.x] = globaltimer_ns();
     const StepConsts kc{p.k_one, p.k_two, p.k_mone};
     uint32_t cols = 0, ld = 0, rd = 0, avail = 0;
     uint32_t sp = my_base, bot = my_base;
@@ -375,6 +377,9 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
             }
         }
     }
+
+    // CTA finish time: the last warp of the CTA to leave the DFS loop.
+    if (p.cta_times) atomicMax(p.cta_times + 2 * blockIdx.x + 1, globaltimer_ns());
 
     // Flush what the last trip left (deadline exit, or the final fold).
     if (PER_OWNER) {

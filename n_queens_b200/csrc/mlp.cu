@@ -1,0 +1,737 @@
+// mlp.cu -- the learned subtree-cost model and the longest-first scheduler.
+//
+// No counterpart in the reference (its tasks run in expander order through
+// one atomic ticket, src/n_queens_cuda.cu:10,80).  A small MLP predicts
+// log2(1 + DFS nodes) of a prefix task from its three masks; the predictions
+// order the task queue longest-first (binned to 1/8 of a log2 unit, stable
+// inside a bin).  The order only changes which lane runs which task, never a
+// count.
+//
+// Model: x (96 bits: cols, ld, rd, each as 32 bits with the columns >= N
+// cleared) -> 128 ReLU -> 128 ReLU -> 1.  Weights are BF16 for compute with
+// FP32 master copies for Adam; biases are FP32; every sum accumulates in
+// FP32.  Kernels (all hand-written, CUDA cores; at 29k parameters the model
+// is far too small for tensor-core tiles to pay):
+//   mlp_predict_kernel  forward for many tasks, 32 tasks per group per CTA
+//   mlp_train_kernel    forward + backward of a minibatch slice; per-CTA
+//                       partial gradients (no atomics: deterministic)
+//   mlp_adam_kernel     sums the partials in CTA order, Adam step, refreshes
+//                       the BF16 copies
+// The first layer exploits binary inputs: h1 = b1 + sum of the W1 columns of
+// the set bits (about 3k of them for a k-row prefix), so no feature matrix
+// is ever materialised.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <cmath>
+#include <cub/device/device_radix_sort.cuh>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "dfs_kernel.cuh"
+#include "expand.h"
+#include "n_queens_b200.h"
+
+namespace nqb {
+
+void set_last_error(const char *msg);
+
+namespace {
+
+constexpr int kIn = 96, kH1 = 128, kH2 = 128;
+// Flat FP32 parameter layout (also the layout of gradients and of
+// nq_mlp_get_params): W1[H1][IN], b1[H1], W2[H2][H1], b2[H2], W3[H2], b3.
+constexpr int kOffW1 = 0;
+constexpr int kOffB1 = kOffW1 + kH1 * kIn;
+constexpr int kOffW2 = kOffB1 + kH1;
+constexpr int kOffB2 = kOffW2 + kH2 * kH1;
+constexpr int kOffW3 = kOffB2 + kH2;
+constexpr int kOffB3 = kOffW3 + kH2;
+constexpr int kParams = kOffB3 + 1;
+constexpr int kGroup = 32;  // tasks per group (one per lane of the layer-3 reduction)
+
+// Compute copy of the weights in device memory.
+struct Weights {
+    __nv_bfloat16 w1t[kIn * kH1];  // [input bit][hidden unit]
+    __nv_bfloat16 w2[kH2 * kH1];   // [unit of layer 2][unit of layer 1]
+    __nv_bfloat16 w3[kH2];
+    float b1[kH1];
+    float b2[kH2];
+    float b3;
+};
+
+struct TaskView {
+    const uint32_t *cols, *ld, *rd;
+    const uint8_t *task_n;  // per-task board size or nullptr
+    const uint32_t *index;  // optional indirection (training permutation)
+    int N;
+};
+
+__device__ __forceinline__ void load_masks(const TaskView &tv, long long t, uint32_t &m0, uint32_t &m1,
+                                           uint32_t &m2) {
+    const long long i = tv.index ? (long long)tv.index[t] : t;
+    const int n = tv.task_n ? (int)tv.task_n[i] : tv.N;
+    const uint32_t last = (n >= 32) ? 0xffffffffu : ((1u << n) - 1u);
+    m0 = tv.cols[i] & last;
+    m1 = tv.ld[i] & last;
+    m2 = tv.rd[i] & last;
+}
+
+// Layer 1 for one task and hidden unit j: b1[j] + sum of W1 columns of the
+// set input bits.  Every thread of the CTA walks the same bits (uniform).
+__device__ __forceinline__ float layer1(const __nv_bfloat16 *w1t, float b, uint32_t m0, uint32_t m1, uint32_t m2,
+                                        int j) {
+    float acc = b;
+    while (m0) {
+        const int f = __ffs(m0) - 1;
+        m0 &= m0 - 1;
+        acc += __bfloat162float(w1t[f * kH1 + j]);
+    }
+    while (m1) {
+        const int f = __ffs(m1) - 1 + 32;
+        m1 &= m1 - 1;
+        acc += __bfloat162float(w1t[f * kH1 + j]);
+    }
+    while (m2) {
+        const int f = __ffs(m2) - 1 + 64;
+        m2 &= m2 - 1;
+        acc += __bfloat162float(w1t[f * kH1 + j]);
+    }
+    return acc;
+}
+
+// Layer 2 pre-activation of unit j for one task: w2row holds W2[j][:] as
+// 64 packed BF16 pairs, h1 the task's 128 layer-1 outputs (broadcast reads).
+__device__ __forceinline__ float layer2(const uint32_t (&w2row)[kH1 / 2], float b, const float *h1) {
+    float acc = b;
+#pragma unroll
+    for (int i = 0; i < kH1; i += 4) {
+        const float4 h = *reinterpret_cast<const float4 *>(h1 + i);
+        const __nv_bfloat162 wa = *reinterpret_cast<const __nv_bfloat162 *>(&w2row[i / 2]);
+        const __nv_bfloat162 wb = *reinterpret_cast<const __nv_bfloat162 *>(&w2row[i / 2 + 1]);
+        acc = fmaf(__low2float(wa), h.x, acc);
+        acc = fmaf(__high2float(wa), h.y, acc);
+        acc = fmaf(__low2float(wb), h.z, acc);
+        acc = fmaf(__high2float(wb), h.w, acc);
+    }
+    return acc;
+}
+
+__device__ __forceinline__ void load_w2row(const Weights *w, int j, uint32_t (&w2row)[kH1 / 2]) {
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(w->w2 + j * kH1);
+#pragma unroll
+    for (int i = 0; i < kH1 / 2; ++i) w2row[i] = src[i];
+}
+
+// Forward over n tasks: out[t] = predicted log2(1 + nodes).  128 threads,
+// thread j = hidden unit j.
+__global__ void __launch_bounds__(128) mlp_predict_kernel(TaskView tv, long long n, const Weights *w, float *out) {
+    __shared__ __align__(16) __nv_bfloat16 s_w1t[kIn * kH1];
+    __shared__ __align__(16) float s_h[kGroup * kH1];
+    __shared__ uint32_t s_m[3][kGroup];
+    const int j = threadIdx.x;
+    for (int i = j; i < kIn * kH1 / 8; i += blockDim.x)
+        reinterpret_cast<uint4 *>(s_w1t)[i] = reinterpret_cast<const uint4 *>(w->w1t)[i];
+    uint32_t w2row[kH1 / 2];
+    load_w2row(w, j, w2row);
+    const float b1 = w->b1[j], b2 = w->b2[j], w3 = __bfloat162float(w->w3[j]), b3 = w->b3;
+    const int warp = j >> 5, lane = j & 31;
+    __syncthreads();
+    for (long long g0 = (long long)blockIdx.x * kGroup; g0 < n; g0 += (long long)gridDim.x * kGroup) {
+        const int gn = (int)min((long long)kGroup, n - g0);
+        if (j < gn) load_masks(tv, g0 + j, s_m[0][j], s_m[1][j], s_m[2][j]);
+        __syncthreads();
+        for (int s = 0; s < gn; ++s)
+            s_h[s * kH1 + j] = fmaxf(layer1(s_w1t, b1, s_m[0][s], s_m[1][s], s_m[2][s], j), 0.f);
+        __syncthreads();
+        float v[kGroup];
+#pragma unroll
+        for (int s = 0; s < kGroup; ++s) v[s] = (s < gn) ? fmaxf(layer2(w2row, b2, s_h + s * kH1), 0.f) * w3 : 0.f;
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < kGroup; ++s) s_h[s * kH1 + j] = v[s];
+        __syncthreads();
+        // layer 3: warp w reduces tasks 8w..8w+7, each lane summing 4 units
+        for (int s = warp * 8; s < warp * 8 + 8; ++s) {
+            const float4 q = *reinterpret_cast<const float4 *>(s_h + s * kH1 + lane * 4);
+            float a = (q.x + q.y) + (q.z + q.w);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+            if (lane == 0 && s < gn) out[g0 + s] = a + b3;
+        }
+        __syncthreads();
+    }
+}
+
+// Shared memory of the training kernel (about 216 KiB; one CTA per SM).
+struct TrainSmem {
+    __nv_bfloat16 w1t[kIn * kH1];    // 24 KiB
+    __nv_bfloat162 w2p[kH2 / 2 * kH1];  // 32 KiB: w2p[(j/2)*H1 + i] = (W2[j][i], W2[j+1][i])
+    float h1[kGroup * kH1];          // 16 KiB: relu(layer 1), [task][unit]
+    float h2[kGroup * kH1];          // 16 KiB: relu(layer 2), then dL/d(pre-act 2)
+    float dh1[kGroup * kH1];         // 16 KiB: dL/d(pre-act 1)
+    float dw1[kIn * kH1];            // 48 KiB: [input bit][unit]
+    float dw2[kH1 * kH2];            // 64 KiB: [unit of layer 1][unit of layer 2]
+    float dout[kGroup];
+    float y[kGroup];
+    uint32_t m[3][kGroup];
+};
+
+// Forward + backward of tasks [begin, end) of the view (mean-squared-error
+// loss with gradient scale `scale` = 2/batch), one partial gradient per CTA.
+__global__ void __launch_bounds__(128, 1)
+    mlp_train_kernel(TaskView tv, const float *target, long long begin, long long end, float scale,
+                     const Weights *w, float *grad_part, float *loss_part) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TrainSmem &S = *reinterpret_cast<TrainSmem *>(smem_raw);
+    const int j = threadIdx.x;  // unit index in every layer (H1 == H2 == blockDim.x)
+    const int warp = j >> 5, lane = j & 31;
+    for (int i = j; i < kIn * kH1 / 8; i += blockDim.x)
+        reinterpret_cast<uint4 *>(S.w1t)[i] = reinterpret_cast<const uint4 *>(w->w1t)[i];
+    for (int jj = 0; jj < kH2; jj += 2)
+        S.w2p[(jj / 2) * kH1 + j] = __halves2bfloat162(w->w2[jj * kH1 + j], w->w2[(jj + 1) * kH1 + j]);
+    for (int i = j; i < kIn * kH1; i += blockDim.x) S.dw1[i] = 0.f;
+    for (int i = j; i < kH1 * kH2; i += blockDim.x) S.dw2[i] = 0.f;
+    uint32_t w2row[kH1 / 2];
+    load_w2row(w, j, w2row);
+    const float b1 = w->b1[j], b2 = w->b2[j], w3 = __bfloat162float(w->w3[j]), b3 = w->b3;
+    float w3q[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) w3q[k] = __bfloat162float(w->w3[lane * 4 + k]);
+    float gb1 = 0.f, gb2 = 0.f, gw3 = 0.f, gb3 = 0.f, loss = 0.f;
+    __syncthreads();
+
+    for (long long g0 = begin + (long long)blockIdx.x * kGroup; g0 < end; g0 += (long long)gridDim.x * kGroup) {
+        const int gn = (int)min((long long)kGroup, end - g0);
+        if (j < kGroup) {
+            if (j < gn) {
+                load_masks(tv, g0 + j, S.m[0][j], S.m[1][j], S.m[2][j]);
+                const long long i = tv.index ? (long long)tv.index[g0 + j] : g0 + j;
+                S.y[j] = target[i];
+            } else {
+                S.m[0][j] = S.m[1][j] = S.m[2][j] = 0;
+                S.y[j] = 0.f;
+            }
+        }
+        __syncthreads();
+        // forward
+        for (int s = 0; s < gn; ++s)
+            S.h1[s * kH1 + j] = fmaxf(layer1(S.w1t, b1, S.m[0][s], S.m[1][s], S.m[2][s], j), 0.f);
+        __syncthreads();
+        for (int s = 0; s < gn; ++s) S.h2[s * kH1 + j] = fmaxf(layer2(w2row, b2, S.h1 + s * kH1), 0.f);
+        __syncthreads();
+        for (int s = warp * 8; s < warp * 8 + 8; ++s) {
+            const float4 q = *reinterpret_cast<const float4 *>(S.h2 + s * kH1 + lane * 4);
+            float a = q.x * w3q[0];
+            a = fmaf(q.y, w3q[1], a);
+            a = fmaf(q.z, w3q[2], a);
+            a = fmaf(q.w, w3q[3], a);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+            if (lane == 0) {
+                const float e = (s < gn) ? (a + b3 - S.y[s]) : 0.f;
+                S.dout[s] = scale * e;
+                loss += e * e;
+            }
+        }
+        __syncthreads();
+        // layer 3 and layer 2 backward (thread j = unit of layer 2)
+        for (int s = 0; s < gn; ++s) {
+            const float h = S.h2[s * kH1 + j];
+            const float d = S.dout[s];
+            gw3 = fmaf(d, h, gw3);
+            const float dh = (h > 0.f) ? d * w3 : 0.f;
+            S.h2[s * kH1 + j] = dh;
+            gb2 += dh;
+        }
+        if (j == 0)
+            for (int s = 0; s < gn; ++s) gb3 += S.dout[s];
+        __syncthreads();
+        // dW2[j][i] += sum_s dh2[s][j] * h1[s][i]   (accumulated as dw2[i][j])
+        for (int i0 = 0; i0 < kH1; i0 += 32) {
+            float acc[32];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) acc[k] = 0.f;
+            for (int s = 0; s < gn; ++s) {
+                const float d = S.h2[s * kH1 + j];
+#pragma unroll
+                for (int k = 0; k < 32; k += 4) {
+                    const float4 h = *reinterpret_cast<const float4 *>(S.h1 + s * kH1 + i0 + k);
+                    acc[k] = fmaf(d, h.x, acc[k]);
+                    acc[k + 1] = fmaf(d, h.y, acc[k + 1]);
+                    acc[k + 2] = fmaf(d, h.z, acc[k + 2]);
+                    acc[k + 3] = fmaf(d, h.w, acc[k + 3]);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 32; ++k) S.dw2[(i0 + k) * kH2 + j] += acc[k];
+        }
+        // dh1[s][i] = relu'(h1) * sum_j W2[j][i] dh2[s][j]   (thread j acts as unit i of layer 1)
+        for (int s = 0; s < gn; ++s) {
+            float acc = 0.f;
+            const float *dh2 = S.h2 + s * kH1;
+#pragma unroll 8
+            for (int jj = 0; jj < kH2; jj += 4) {
+                const float4 d = *reinterpret_cast<const float4 *>(dh2 + jj);
+                const __nv_bfloat162 wa = S.w2p[(jj / 2) * kH1 + j];
+                const __nv_bfloat162 wb = S.w2p[(jj / 2 + 1) * kH1 + j];
+                acc = fmaf(__low2float(wa), d.x, acc);
+                acc = fmaf(__high2float(wa), d.y, acc);
+                acc = fmaf(__low2float(wb), d.z, acc);
+                acc = fmaf(__high2float(wb), d.w, acc);
+            }
+            const float dh = (S.h1[s * kH1 + j] > 0.f) ? acc : 0.f;
+            S.dh1[s * kH1 + j] = dh;
+            gb1 += dh;
+        }
+        __syncthreads();
+        // dW1[i][f] += sum_s dh1[s][i] over the set bits f of task s
+        for (int s = 0; s < gn; ++s) {
+            const float d = S.dh1[s * kH1 + j];
+            uint32_t m0 = S.m[0][s], m1 = S.m[1][s], m2 = S.m[2][s];
+            while (m0) {
+                const int f = __ffs(m0) - 1;
+                m0 &= m0 - 1;
+                S.dw1[f * kH1 + j] += d;
+            }
+            while (m1) {
+                const int f = __ffs(m1) - 1 + 32;
+                m1 &= m1 - 1;
+                S.dw1[f * kH1 + j] += d;
+            }
+            while (m2) {
+                const int f = __ffs(m2) - 1 + 64;
+                m2 &= m2 - 1;
+                S.dw1[f * kH1 + j] += d;
+            }
+        }
+        __syncthreads();
+    }
+
+    // Partial gradient of this CTA in the flat parameter layout.
+    float *g = grad_part + (size_t)blockIdx.x * kParams;
+    for (int f = 0; f < kIn; ++f) g[kOffW1 + j * kIn + f] = S.dw1[f * kH1 + j];
+    g[kOffB1 + j] = gb1;
+    for (int i = 0; i < kH1; ++i) g[kOffW2 + j * kH1 + i] = S.dw2[i * kH2 + j];
+    g[kOffB2 + j] = gb2;
+    g[kOffW3 + j] = gw3;
+    if (j == 0) g[kOffB3] = gb3;
+    // loss: lanes 0 of each warp hold partial sums
+    __shared__ float s_loss[4];
+    if (lane == 0) s_loss[warp] = loss;
+    __syncthreads();
+    if (j == 0) loss_part[blockIdx.x] = (s_loss[0] + s_loss[1]) + (s_loss[2] + s_loss[3]);
+}
+
+// Master weights -> compute copy (round to nearest even BF16).
+__device__ __forceinline__ void refresh_one(int p, float v, Weights *w) {
+    if (p < kOffB1) {
+        const int i = (p - kOffW1) / kIn, f = (p - kOffW1) % kIn;
+        w->w1t[f * kH1 + i] = __float2bfloat16_rn(v);
+    } else if (p < kOffW2) {
+        w->b1[p - kOffB1] = v;
+    } else if (p < kOffB2) {
+        w->w2[p - kOffW2] = __float2bfloat16_rn(v);
+    } else if (p < kOffW3) {
+        w->b2[p - kOffB2] = v;
+    } else if (p < kOffB3) {
+        w->w3[p - kOffW3] = __float2bfloat16_rn(v);
+    } else {
+        w->b3 = v;
+    }
+}
+
+__global__ void mlp_refresh_kernel(const float *master, Weights *w) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < kParams; p += gridDim.x * blockDim.x)
+        refresh_one(p, master[p], w);
+}
+
+// Sums the per-CTA partial gradients in CTA order (deterministic), applies
+// one Adam step to the master weights and refreshes the compute copy.
+// nparts == 0 only sums (gradient check): grad_out receives the gradient.
+__global__ void mlp_adam_kernel(float *master, float *m1, float *m2, const float *grad_part, int nparts,
+                                float lr, float beta1, float beta2, float eps, float bc1, float bc2, Weights *w,
+                                float *grad_out, int apply) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < kParams; p += gridDim.x * blockDim.x) {
+        float g = 0.f;
+        for (int b = 0; b < nparts; ++b) g += grad_part[(size_t)b * kParams + p];
+        if (grad_out) grad_out[p] = g;
+        if (!apply) continue;
+        const float a = beta1 * m1[p] + (1.f - beta1) * g;
+        const float v = beta2 * m2[p] + (1.f - beta2) * g * g;
+        m1[p] = a;
+        m2[p] = v;
+        const float upd = (a / bc1) / (sqrtf(v / bc2) + eps);
+        const float nw = master[p] - lr * upd;
+        master[p] = nw;
+        refresh_one(p, nw, w);
+    }
+}
+
+// Sort keys for the longest-first order: predicted log2 cost in 1/8 units.
+__global__ void mlp_bin_kernel(const float *pred, long long n, uint16_t *key, uint32_t *idx) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const float v = fminf(fmaxf(pred[t] * 8.f + 0.5f, 0.f), 65535.f);
+        key[t] = (uint16_t)v;
+        idx[t] = (uint32_t)t;
+    }
+}
+
+}  // namespace
+}  // namespace nqb
+
+using namespace nqb;
+
+struct nq_mlp {
+    std::mutex mu;
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    float *master = nullptr, *adam1 = nullptr, *adam2 = nullptr;
+    Weights *w = nullptr;
+    long long steps = 0;
+    // scratch
+    float *grad_part = nullptr;
+    int grad_parts_cap = 0;
+    float *gsum = nullptr;  // summed gradient (nq_mlp_grad)
+    float *loss_part = nullptr;
+    void *data = nullptr;
+    size_t data_cap = 0;
+    void *sort_tmp = nullptr;
+    size_t sort_tmp_cap = 0;
+};
+
+namespace {
+
+int mlp_fail(cudaError_t e, const char *what) {
+    set_last_error((std::string(what) + ": " + cudaGetErrorString(e)).c_str());
+    (void)cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? NQ_ERR_OOM : NQ_ERR_CUDA;
+}
+
+#define MLP_CUDA(call)                                          \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return mlp_fail(e_, #call);      \
+    } while (0)
+
+int grow(void *&p, size_t &cap, size_t need) {
+    if (need <= cap) return NQ_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = need + need / 4 + 256;
+    MLP_CUDA(cudaMalloc(&p, want));
+    cap = want;
+    return NQ_OK;
+}
+
+int train_blocks(nq_mlp *m) { return m->sms; }
+
+uint64_t splitmix(uint64_t &s) {
+    s += 0x9E3779B97F4A7C15ull;
+    uint64_t z = s;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Uploads a task list (+ per-task N and targets) into the model's scratch:
+// [cols | ld | rd | index] u32, [target] f32, [task_n] u8.
+struct Staged {
+    uint32_t *cols, *ld, *rd, *index;
+    float *target;
+    uint8_t *task_n;
+};
+
+int stage(nq_mlp *m, const uint8_t *task_n, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd,
+          const float *target, int64_t n, Staged &st) {
+    const size_t need = (size_t)n * (4 * 4 + 4 + 1) + 1024;
+    int rc = grow(m->data, m->data_cap, need);
+    if (rc) return rc;
+    char *b = (char *)m->data;
+    st.cols = (uint32_t *)b;
+    st.ld = st.cols + n;
+    st.rd = st.ld + n;
+    st.index = st.rd + n;
+    st.target = (float *)(st.index + n);
+    st.task_n = (uint8_t *)(st.target + n);
+    MLP_CUDA(cudaMemcpyAsync(st.cols, cols, (size_t)n * 4, cudaMemcpyHostToDevice, m->stream));
+    MLP_CUDA(cudaMemcpyAsync(st.ld, ld, (size_t)n * 4, cudaMemcpyHostToDevice, m->stream));
+    MLP_CUDA(cudaMemcpyAsync(st.rd, rd, (size_t)n * 4, cudaMemcpyHostToDevice, m->stream));
+    if (target) MLP_CUDA(cudaMemcpyAsync(st.target, target, (size_t)n * 4, cudaMemcpyHostToDevice, m->stream));
+    if (task_n) MLP_CUDA(cudaMemcpyAsync(st.task_n, task_n, (size_t)n, cudaMemcpyHostToDevice, m->stream));
+    return NQ_OK;
+}
+
+int ensure_grad_parts(nq_mlp *m, int parts) {
+    if (parts <= m->grad_parts_cap) return NQ_OK;
+    if (m->grad_part) cudaFree(m->grad_part);
+    if (m->loss_part) cudaFree(m->loss_part);
+    m->grad_part = nullptr;
+    m->loss_part = nullptr;
+    MLP_CUDA(cudaMalloc(&m->grad_part, (size_t)parts * kParams * sizeof(float)));
+    MLP_CUDA(cudaMalloc(&m->loss_part, (size_t)parts * sizeof(float)));
+    m->grad_parts_cap = parts;
+    return NQ_OK;
+}
+
+// One forward+backward over [begin, end) into the partials; returns #parts.
+int launch_train(nq_mlp *m, const TaskView &tv, const float *target, long long begin, long long end, float scale,
+                 int &parts) {
+    // Two groups of 32 tasks per CTA amortise the CTA's weight load and its
+    // partial-gradient write; at most one CTA per SM (the kernel takes ~216 KiB).
+    const long long groups = (end - begin + kGroup - 1) / kGroup;
+    parts = (int)std::min<long long>(train_blocks(m), std::max<long long>((groups + 1) / 2, 1));
+    int rc = ensure_grad_parts(m, parts);
+    if (rc) return rc;
+    mlp_train_kernel<<<parts, kH1, sizeof(TrainSmem), m->stream>>>(tv, target, begin, end, scale, m->w,
+                                                                    m->grad_part, m->loss_part);
+    MLP_CUDA(cudaGetLastError());
+    return NQ_OK;
+}
+
+int check_model(nq_mlp *m) {
+    if (!m) return NQ_ERR_ARG;
+    MLP_CUDA(cudaSetDevice(m->device));
+    return NQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nq_mlp_num_params(void) { return kParams; }
+
+int nq_mlp_create(int device, uint64_t seed, nq_mlp **out) {
+    if (!out) return NQ_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        (void)cudaGetLastError();
+        set_last_error("no CUDA device");
+        return NQ_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return NQ_ERR_ARG;
+    MLP_CUDA(cudaSetDevice(device));
+    nq_mlp *m = new nq_mlp();
+    m->device = device;
+    cudaDeviceGetAttribute(&m->sms, cudaDevAttrMultiProcessorCount, device);
+    cudaError_t e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&m->master, kParams * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&m->adam1, kParams * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&m->adam2, kParams * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&m->w, sizeof(Weights));
+    if (e == cudaSuccess) e = cudaMalloc(&m->gsum, kParams * sizeof(float));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sizeof(TrainSmem));
+    if (e != cudaSuccess) {
+        nq_mlp_destroy(m);
+        return mlp_fail(e, "nq_mlp_create");
+    }
+    // Uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) for every weight and bias,
+    // from SplitMix64(seed).
+    std::vector<float> p(kParams);
+    uint64_t s = seed;
+    auto uni = [&](float bound) {
+        const double u = (double)(splitmix(s) >> 11) * (1.0 / 9007199254740992.0);
+        return (float)((2.0 * u - 1.0) * bound);
+    };
+    for (int i = kOffW1; i < kOffB1; ++i) p[i] = uni(1.f / std::sqrt((float)kIn));
+    for (int i = kOffB1; i < kOffW2; ++i) p[i] = uni(1.f / std::sqrt((float)kIn));
+    for (int i = kOffW2; i < kOffB2; ++i) p[i] = uni(1.f / std::sqrt((float)kH1));
+    for (int i = kOffB2; i < kOffW3; ++i) p[i] = uni(1.f / std::sqrt((float)kH1));
+    for (int i = kOffW3; i < kOffB3; ++i) p[i] = uni(1.f / std::sqrt((float)kH2));
+    p[kOffB3] = uni(1.f / std::sqrt((float)kH2));
+    *out = m;
+    return nq_mlp_set_params(m, p.data());
+}
+
+int nq_mlp_destroy(nq_mlp *m) {
+    if (!m) return NQ_OK;
+    cudaSetDevice(m->device);
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    cudaFree(m->master);
+    cudaFree(m->adam1);
+    cudaFree(m->adam2);
+    cudaFree(m->w);
+    cudaFree(m->gsum);
+    cudaFree(m->grad_part);
+    cudaFree(m->loss_part);
+    cudaFree(m->data);
+    cudaFree(m->sort_tmp);
+    if (m->stream) cudaStreamDestroy(m->stream);
+    delete m;
+    return NQ_OK;
+}
+
+int nq_mlp_get_params(nq_mlp *m, float *out) {
+    int rc = check_model(m);
+    if (rc) return rc;
+    if (!out) return NQ_ERR_ARG;
+    std::lock_guard<std::mutex> lock(m->mu);
+    MLP_CUDA(cudaMemcpyAsync(out, m->master, kParams * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+    MLP_CUDA(cudaStreamSynchronize(m->stream));
+    return NQ_OK;
+}
+
+int nq_mlp_set_params(nq_mlp *m, const float *in) {
+    int rc = check_model(m);
+    if (rc) return rc;
+    if (!in) return NQ_ERR_ARG;
+    std::lock_guard<std::mutex> lock(m->mu);
+    MLP_CUDA(cudaMemcpyAsync(m->master, in, kParams * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+    MLP_CUDA(cudaMemsetAsync(m->adam1, 0, kParams * sizeof(float), m->stream));
+    MLP_CUDA(cudaMemsetAsync(m->adam2, 0, kParams * sizeof(float), m->stream));
+    mlp_refresh_kernel<<<(kParams + 255) / 256, 256, 0, m->stream>>>(m->master, m->w);
+    MLP_CUDA(cudaGetLastError());
+    MLP_CUDA(cudaStreamSynchronize(m->stream));
+    m->steps = 0;
+    return NQ_OK;
+}
+
+int nq_mlp_predict(nq_mlp *m, int N, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd, int64_t n,
+                   float *out) {
+    int rc = check_model(m);
+    if (rc) return rc;
+    if (N < 1 || N > NQ_MAX_N || n < 0 || (n > 0 && (!cols || !ld || !rd || !out))) return NQ_ERR_ARG;
+    if (n == 0) return NQ_OK;
+    std::lock_guard<std::mutex> lock(m->mu);
+    Staged st;
+    rc = stage(m, nullptr, cols, ld, rd, nullptr, n, st);
+    if (rc) return rc;
+    TaskView tv{st.cols, st.ld, st.rd, nullptr, nullptr, N};
+    float *d_out = st.target;
+    const int grid = (int)std::min<long long>((n + kGroup - 1) / kGroup, (long long)m->sms * 8);
+    mlp_predict_kernel<<<grid, kH1, 0, m->stream>>>(tv, n, m->w, d_out);
+    MLP_CUDA(cudaGetLastError());
+    MLP_CUDA(cudaMemcpyAsync(out, d_out, (size_t)n * 4, cudaMemcpyDeviceToHost, m->stream));
+    MLP_CUDA(cudaStreamSynchronize(m->stream));
+    return NQ_OK;
+}
+
+int nq_mlp_grad(nq_mlp *m, const uint8_t *task_n, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd,
+                const float *target, int64_t n, float *grad_out, float *loss_out) {
+    int rc = check_model(m);
+    if (rc) return rc;
+    if (n <= 0 || !task_n || !cols || !ld || !rd || !target || !grad_out) return NQ_ERR_ARG;
+    std::lock_guard<std::mutex> lock(m->mu);
+    Staged st;
+    rc = stage(m, task_n, cols, ld, rd, target, n, st);
+    if (rc) return rc;
+    TaskView tv{st.cols, st.ld, st.rd, st.task_n, nullptr, 0};
+    int parts = 0;
+    rc = launch_train(m, tv, st.target, 0, n, 2.f / (float)n, parts);
+    if (rc) return rc;
+    mlp_adam_kernel<<<(kParams + 255) / 256, 256, 0, m->stream>>>(m->master, m->adam1, m->adam2, m->grad_part,
+                                                                  parts, 0.f, 0.f, 0.f, 0.f, 1.f, 1.f, m->w, m->gsum, 0);
+    cudaError_t e = cudaGetLastError();
+    std::vector<float> lp(parts);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(grad_out, m->gsum, kParams * sizeof(float), cudaMemcpyDeviceToHost, m->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(lp.data(), m->loss_part, parts * sizeof(float), cudaMemcpyDeviceToHost, m->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+    if (e != cudaSuccess) return mlp_fail(e, "nq_mlp_grad");
+    if (loss_out) {
+        double l = 0;
+        for (float v : lp) l += v;
+        *loss_out = (float)(l / (double)n);
+    }
+    return NQ_OK;
+}
+
+int nq_mlp_train(nq_mlp *m, const uint8_t *task_n, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd,
+                 const float *target, int64_t n, int epochs, int batch, float lr, uint64_t seed,
+                 float *epoch_loss) {
+    int rc = check_model(m);
+    if (rc) return rc;
+    if (n <= 0 || !task_n || !cols || !ld || !rd || !target || epochs < 0 || batch < kGroup || lr <= 0.f)
+        return NQ_ERR_ARG;
+    if (n > 0xffffffffll) return NQ_ERR_ARG;
+    std::lock_guard<std::mutex> lock(m->mu);
+    Staged st;
+    rc = stage(m, task_n, cols, ld, rd, target, n, st);
+    if (rc) return rc;
+    std::vector<uint32_t> perm((size_t)n);
+    uint64_t s = seed;
+    const int parts_max = train_blocks(m);
+    rc = ensure_grad_parts(m, parts_max);
+    if (rc) return rc;
+    const long long nsteps_epoch = (n + batch - 1) / batch;
+    std::vector<float> lp((size_t)parts_max * nsteps_epoch);
+    for (int ep = 0; ep < epochs; ++ep) {
+        // Fisher-Yates shuffle from SplitMix64(seed), one per epoch.
+        for (int64_t i = 0; i < n; ++i) perm[i] = (uint32_t)i;
+        for (int64_t i = n - 1; i > 0; --i) {
+            const int64_t k = (int64_t)(splitmix(s) % (uint64_t)(i + 1));
+            std::swap(perm[i], perm[k]);
+        }
+        MLP_CUDA(cudaMemcpyAsync(st.index, perm.data(), (size_t)n * 4, cudaMemcpyHostToDevice, m->stream));
+        TaskView tv{st.cols, st.ld, st.rd, st.task_n, st.index, 0};
+        double eloss = 0;
+        for (long long b0 = 0, stepi = 0; b0 < n; b0 += batch, ++stepi) {
+            const long long b1 = std::min<long long>(n, b0 + batch);
+            int parts = 0;
+            rc = launch_train(m, tv, st.target, b0, b1, 2.f / (float)(b1 - b0), parts);
+            if (rc) return rc;
+            m->steps += 1;
+            const float bc1 = 1.f - std::pow(0.9f, (float)m->steps);
+            const float bc2 = 1.f - std::pow(0.999f, (float)m->steps);
+            mlp_adam_kernel<<<(kParams + 255) / 256, 256, 0, m->stream>>>(m->master, m->adam1, m->adam2,
+                                                                          m->grad_part, parts, lr, 0.9f, 0.999f,
+                                                                          1e-8f, bc1, bc2, m->w, nullptr, 1);
+            MLP_CUDA(cudaGetLastError());
+            if (epoch_loss)
+                MLP_CUDA(cudaMemcpyAsync(lp.data() + (size_t)stepi * parts_max, m->loss_part, parts * sizeof(float),
+                                         cudaMemcpyDeviceToHost, m->stream));
+            if (epoch_loss && parts < parts_max)
+                for (int q = parts; q < parts_max; ++q) lp[(size_t)stepi * parts_max + q] = 0.f;
+        }
+        if (epoch_loss) {
+            MLP_CUDA(cudaStreamSynchronize(m->stream));
+            for (float v : lp) eloss += v;
+            epoch_loss[ep] = (float)(eloss / (double)n);
+        }
+    }
+    MLP_CUDA(cudaStreamSynchronize(m->stream));
+    return NQ_OK;
+}
+
+// Longest-first order of device-resident tasks: predictions -> keys in
+// 1/8-log2 bins -> stable descending radix sort of task indices.
+int nq_schedule_device(nq_mlp *m, int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd,
+                       int64_t n, uint32_t *d_order, float *d_pred, void *stream) {
+    int rc = check_model(m);
+    if (rc) return rc;
+    if (N < 1 || N > NQ_MAX_N || n < 0 || n > 0xffffffffll || (n > 0 && (!d_cols || !d_ld || !d_rd || !d_order)))
+        return NQ_ERR_ARG;
+    if (n == 0) return NQ_OK;
+    std::lock_guard<std::mutex> lock(m->mu);
+    cudaStream_t s = stream ? (cudaStream_t)stream : m->stream;
+    // scratch: pred f32 | key u16 | key_out u16 | idx u32
+    const size_t need = (size_t)n * (4 + 2 + 2 + 4) + 1024;
+    rc = grow(m->data, m->data_cap, need);
+    if (rc) return rc;
+    float *pred = d_pred ? d_pred : (float *)m->data;
+    uint16_t *key = (uint16_t *)((char *)m->data + (size_t)n * 4);
+    uint16_t *key2 = key + n;
+    uint32_t *idx = (uint32_t *)(((uintptr_t)(key2 + n) + 15) & ~(uintptr_t)15);
+    TaskView tv{d_cols, d_ld, d_rd, nullptr, nullptr, N};
+    const int grid = (int)std::min<long long>((n + kGroup - 1) / kGroup, (long long)m->sms * 8);
+    mlp_predict_kernel<<<grid, kH1, 0, s>>>(tv, n, m->w, pred);
+    MLP_CUDA(cudaGetLastError());
+    mlp_bin_kernel<<<m->sms * 4, 256, 0, s>>>(pred, n, key, idx);
+    MLP_CUDA(cudaGetLastError());
+    size_t tmp = 0;
+    MLP_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, key, key2, idx, d_order, (int)n, 0, 16, s));
+    rc = grow(m->sort_tmp, m->sort_tmp_cap, tmp);
+    if (rc) return rc;
+    MLP_CUDA(cub::DeviceRadixSort::SortPairsDescending(m->sort_tmp, tmp, key, key2, idx, d_order, (int)n, 0, 16, s));
+    return NQ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,134 @@
+"""The learned subtree-cost scheduler on the GPU: the hand-written MLP kernels
+against the CPU oracle (oracle/mlp_ref.py), training, the longest-first
+order, exact counts with that order, and what the order gains."""
+import numpy as np
+import pytest
+
+import oracle
+from oracle import mlp_ref
+
+pytestmark = pytest.mark.gpu
+
+# Tolerances: the GPU accumulates in FP32 (different summation order), the
+# oracle in float64, both with the same BF16-rounded weights.
+GRAD_RTOL_MAX = 2e-3      # max |g_gpu - g_ref| <= 2e-3 * max |g_ref|
+GRAD_RTOL_L2 = 2e-4       # ||g_gpu - g_ref|| <= 2e-4 * ||g_ref||
+PRED_ATOL = 2e-3          # |pred_gpu - pred_ref| for outputs of size ~10
+
+
+def _params(seed):
+    rng = np.random.default_rng(seed)
+    p = rng.uniform(-0.15, 0.15, mlp_ref.NPARAMS).astype(np.float32)
+    p[mlp_ref.OFF_B1:mlp_ref.OFF_W2] += 0.05
+    p[mlp_ref.OFF_B2:mlp_ref.OFF_W3] += 0.05
+    p[mlp_ref.OFF_B3] = 10.0
+    return p
+
+
+def _mixed_tasks():
+    cs, ls, rs, ns = [], [], [], []
+    for N, k in ((12, 4), (13, 5), (15, 3)):
+        c, l, r = oracle.expand(N, k)
+        sel = np.random.default_rng(N).choice(c.size, min(400, c.size), replace=False)
+        cs.append(c[sel]); ls.append(l[sel]); rs.append(r[sel]); ns.append(np.full(sel.size, N, np.uint8))
+    return np.concatenate(ns), np.concatenate(cs), np.concatenate(ls), np.concatenate(rs)
+
+
+def test_gradients_match_cpu_oracle(gpu):
+    from n_queens_b200 import learned
+    tn, c, l, r = _mixed_tasks()
+    y = np.random.default_rng(3).uniform(4, 16, c.size).astype(np.float32)
+    m = learned.CostModel(seed=5)
+    for seed in (1, 2):
+        p = _params(seed)
+        m.set_params(p)
+        g, loss = m.grad(tn, c, l, r, y)
+        X = np.concatenate([mlp_ref.features(int(N), c[tn == N], l[tn == N], r[tn == N]) for N in np.unique(tn)])
+        order = np.concatenate([np.flatnonzero(tn == N) for N in np.unique(tn)])
+        ref_loss, ref_g = mlp_ref.loss_and_grad(p, X, y[order])
+        assert abs(loss - ref_loss) <= 1e-5 * ref_loss
+        err = np.abs(g.astype(np.float64) - ref_g)
+        assert err.max() <= GRAD_RTOL_MAX * np.abs(ref_g).max()
+        assert np.linalg.norm(err) <= GRAD_RTOL_L2 * np.linalg.norm(ref_g)
+    m.close()
+
+
+def test_predictions_match_cpu_oracle(gpu):
+    from n_queens_b200 import learned
+    m = learned.CostModel(seed=5)
+    p = _params(4)
+    m.set_params(p)
+    for N, k in ((12, 4), (16, 5)):
+        c, l, r = oracle.expand(N, k)
+        c, l, r = c[:3000], l[:3000], r[:3000]
+        got = m.predict(N, c, l, r)
+        want, _ = mlp_ref.forward(p, mlp_ref.features(N, c, l, r))
+        assert np.abs(got - want).max() <= PRED_ATOL
+    assert np.array_equal(m.params(), p)
+    m.close()
+
+
+def test_training_lowers_loss_and_ranks_tasks(gpu):
+    from n_queens_b200 import learned
+    c, l, r, y, nodes, _ = learned.solver_labels(15, 5)
+    assert np.array_equal(nodes, oracle.count_tasks(15, c, l, r, nodes=True)[1])
+    tn = np.full(c.size, 15, np.uint8)
+    m = learned.CostModel(seed=11)
+    p = m.params(); p[-1] = float(y.mean()); m.set_params(p)
+    g0, loss0 = m.grad(tn, c, l, r, y)
+    losses = m.train(tn, c, l, r, y, epochs=6, batch=1024, lr=2e-3, seed=3)
+    _, loss1 = m.grad(tn, c, l, r, y)
+    assert loss1 < 0.5 * loss0 and losses[-1] < losses[0]
+    assert learned.spearman(m.predict(15, c, l, r), y) > 0.6
+    m.close()
+
+
+def test_schedule_is_a_longest_first_permutation(gpu):
+    import torch
+    from n_queens_b200 import learned
+    m = learned.CostModel(seed=2)
+    m.set_params(_params(6))
+    c, l, r = oracle.expand(16, 5)
+    dev = torch.device("cuda:0")
+    tc, tl, tr = (torch.from_numpy(a.view(np.int32)).to(dev) for a in (c, l, r))  # keep them alive
+    order = torch.empty(c.size, dtype=torch.int32, device=dev)
+    pred = torch.empty(c.size, dtype=torch.float32, device=dev)
+    rc = learned.lib.nq_schedule_device(m._m, 16, tc.data_ptr(), tl.data_ptr(), tr.data_ptr(), c.size,
+                                        order.data_ptr(), pred.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert rc == 0
+    torch.cuda.synchronize()
+    o = order.cpu().numpy().view(np.uint32).astype(np.int64)
+    pr = pred.cpu().numpy()
+    assert np.array_equal(np.sort(o), np.arange(c.size))
+    keys = np.clip(np.floor(pr * 8 + 0.5), 0, 65535).astype(np.int64)[o]
+    assert np.all(np.diff(keys) <= 0)                      # longest first
+    same = np.diff(keys) == 0
+    assert np.all(np.diff(o)[same] > 0)                    # stable inside a bin
+    assert np.allclose(pr, m.predict(16, c, l, r), atol=1e-5)
+    m.close()
+
+
+def test_learned_count_is_exact_and_front_loads_work(gpu, golden):
+    from n_queens_b200 import learned
+    pub = golden("published.json")
+    model, rep = learned.build_cost_model(18, k=6, train_N=(14, 15, 16), finetune_frac=0.05, seed=1,
+                                          pre_epochs=3, ft_epochs=8, batch=2048, holdout=100_000)
+    assert rep.holdout_spearman > 0.4, rep
+    for N, k in ((16, 5), (17, 6), (18, 6)):
+        res = learned.count_learned(N, k, model, config=dict(timing=1))
+        assert res.total == pub[str(N)]["total"]
+        assert res.stats["schedule_ms"] > 0
+    # What the network buys: the share of all DFS work that sits in the first
+    # fifth of the queue, in the order the model chose versus expander order.
+    c, l, r, y, nodes, _ = learned.solver_labels(18, 6)
+    pred = model.predict(18, c, l, r)
+    keys = np.clip(np.floor(pred * 8 + 0.5), 0, 65535)
+    order = np.lexsort((np.arange(c.size), -keys))
+    head = c.size // 5
+    share_plain = nodes[:head].sum() / nodes.sum()
+    share_learned = nodes[order[:head]].sum() / nodes.sum()
+    share_oracle = np.sort(nodes)[::-1][:head].sum() / nodes.sum()
+    print(f"work in the first fifth of the queue: plain {share_plain:.3f}, learned {share_learned:.3f}, "
+          f"oracle {share_oracle:.3f}")
+    assert share_learned > share_plain + 0.15
+    model.close()
