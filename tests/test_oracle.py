@@ -109,3 +109,32 @@ def test_oracle_expander_equals_reference_live():
             c, l, r = oracle.expand(N, k)
             ref = oracle.ref_expand_aos(N, k)
             assert np.array_equal(np.stack([c, l, r], axis=1).view(np.int32), ref), (N, k)
+
+
+def test_batch_fixture_against_oracle_and_published(golden):
+    # The 4096-board fixture (reference n_queens() on every distinct board):
+    # its instances replay from the seed, cheap boards agree with the oracle,
+    # empty boards carry the published totals, and where every one-queen
+    # board of an N is present their counts add up to the published total
+    # (the row-0 decomposition).
+    g = golden("boards_4096.json")
+    pub = golden("published.json")
+    assert [list(b) for b in workloads.random_boards(g["n"], g["seed"], *g["N_range"], *g["m_range"])] == \
+        g["instances"]
+    one_queen = {}
+    cheap = []
+    for (N, c, l, r), want in zip(g["instances"], g["counts"]):
+        m = bin(c).count("1")
+        if m == 0 and str(N) in pub:
+            assert want == pub[str(N)]["total"]
+        if m == 1:
+            one_queen.setdefault(N, {})[c] = want
+        if N <= 13 or (N <= 15 and m >= 2):
+            cheap.append((N, c, l, r, want))
+    for N, c, l, r, want in cheap:
+        assert oracle.count_task(N, c, l, r) == want
+    full = [N for N, d in one_queen.items() if len(d) == N]
+    assert 20 in full
+    for N in full:
+        if str(N) in pub:
+            assert sum(one_queen[N].values()) == pub[str(N)]["total"], N
