@@ -7,12 +7,19 @@ persistent DFS kernel, and the step's count is checked bit-exact against the
 reference's published total (README.md / logs).  The default workload is
 N=21, k=6 (4,470,757 prefix tasks).
 
+Two queue orders are timed, interleaved step by step: the learned
+longest-first order (the default headline: an MLP cost model built once per
+run from solver-logged node counts, then a device-side predict + sort inside
+every step) and the plain dynamic fetch in expander order (`compare`).
+
 Reported (one JSON line from rank 0):
-  value      DFS nodes/s with the tasks resident in HBM (kernel + queue reset,
-             CUDA events on the launching stream, L2 flushed between steps);
-  e2e        the same metric through the public C ABI call nq_count (host
-             expansion, pinned H2D copy of the tasks, kernel, D2H of the
-             result), host wall clock per step;
+  value      DFS nodes/s with the tasks resident in HBM (schedule + queue
+             reset + kernel, CUDA events on the launching stream, L2 flushed
+             between steps);
+  e2e        the same metric through the public API (learned:
+             nq_count_learned; plain: nq_count): host expansion, pinned H2D
+             copy of the tasks, schedule, kernel, D2H of the result; host wall
+             clock per step;
   roofline   integer-issue roofline: 22 warp-issue slots per DFS node against
              numSMs x 4 schedulers x clock;
   cpu_baseline  the reference's own CPU recursion (oracle/_ref, all host
@@ -60,13 +67,16 @@ WORKLOADS = {
 def parse_args():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="n21k6")
     ap.add_argument("--cpu-seconds", type=float, default=8.0, help="CPU work per reference-sample step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--schedule", choices=["learned", "plain"], default="learned",
+                    help="queue order of the headline arm; the other order is timed beside it")
+    ap.add_argument("--no-compare", action="store_true", help="skip timing the other queue order")
     return ap.parse_args()
 
 
@@ -300,43 +310,85 @@ def run_ours(args, world, rank, local):
         assert r.total == want, (r.total, want)
         nodes = r.nodes
 
+    # Learned longest-first order: the cost model is built once (solver-logged
+    # labels at N=16..18, fine-tuning on a seeded 5% sample of this board);
+    # every learned step then predicts + sorts on the device and counts.
+    model, build = None, None
+    order = torch.empty(ntasks, dtype=torch.int32, device=dev)
+    lcfg = nq.Config()
+    lcfg.device = local
+    lcfg.stack_levels = levels
+    lcfg.order_kind = nq.NQ_ORDER_GIVEN
+    lcfg.order = order.data_ptr()
+    want_learned = args.schedule == "learned" or not args.no_compare
+    if want_learned:
+        from n_queens_b200 import learned
+        t0 = time.perf_counter()
+        model, rep = learned.build_cost_model(N, k=k, seed=1, device=local)
+        build = {"wall_s": time.perf_counter() - t0, "label_s": rep.label_s, "pretrain_s": rep.pretrain_s,
+                 "finetune_label_s": rep.finetune_label_s, "finetune_s": rep.finetune_s,
+                 "train_samples": rep.train_samples, "finetune_samples": rep.finetune_samples,
+                 "holdout_spearman": rep.holdout_spearman, "holdout_rmse_log2": rep.holdout_rmse}
+
     def check(nsteps):
         s = sums[:nsteps].cpu().numpy()
         for i in range(nsteps):
             if 2 * int(s[i, 0]) != want or int(s[i, 1]) != 0:
                 raise SystemExit(f"step {i}: count {2 * int(s[i, 0])} status {int(s[i, 1])}, want {want}")
 
-    def step(i):
+    def step(i, kind, mid=None):
         sp = sums[i]
+        c = cfg
+        if kind == "learned":
+            rc = learned.lib.nq_schedule_device(model._m, N, tc.data_ptr(), tl.data_ptr(), tr.data_ptr(), ntasks,
+                                                order.data_ptr(), None, stream.cuda_stream)
+            if rc != 0:
+                raise SystemExit(f"nq_schedule_device: {nq.status_string(rc)} {nq.last_error()}")
+            c = lcfg
+        if mid is not None:
+            mid.record(stream)
         rc = nq.lib.nq_count_tasks_device(N, tc.data_ptr(), tl.data_ptr(), tr.data_ptr(), ntasks, None, None,
-                                          sp.data_ptr(), nq.ctypes.byref(cfg), stream.cuda_stream)
+                                          sp.data_ptr(), nq.ctypes.byref(c), stream.cuda_stream)
         if rc != 0:
             raise SystemExit(f"nq_count_tasks_device: {nq.status_string(rc)} {nq.last_error()}")
 
+    head = args.schedule
+    other = None if args.no_compare else ("plain" if head == "learned" else "learned")
     for i in range(args.warmup):
         flush.zero_()
-        step(i)
+        step(i, head)
     torch.cuda.synchronize()
     check(args.warmup)
 
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    # Timed: the headline order and (interleaved, same conditions) the other.
+    arms = [head] + ([other] if other else [])
+    ev = {a: [tuple(torch.cuda.Event(enable_timing=True) for _ in range(3)) for _ in range(args.steps)]
+          for a in arms}
     barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(gpu_uuid) as clk:
         for i in range(args.steps):
-            flush.zero_()
-            starts[i].record(stream)
-            step(i)
-            ends[i].record(stream)
-        torch.cuda.synchronize()
+            for a in arms:
+                flush.zero_()
+                ev[a][i][0].record(stream)
+                step(i, a, mid=ev[a][i][1])
+                ev[a][i][2].record(stream)
+            torch.cuda.synchronize()
+            check(i + 1)
     barrier(world)
     clocks = clk.summary()
-    check(args.steps)
-    kern_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    t_local = sum(kern_ms) / 1000.0
+    arm_s = {a: sum(s.elapsed_time(e) for s, _, e in ev[a]) / 1000.0 for a in arms}
+    dfs_s = sum(m.elapsed_time(e) for _, m, e in ev[head]) / 1000.0  # the DFS kernel alone
+    sched_ms = (arm_s[head] - dfs_s) * 1000.0 / args.steps
+    t_local = arm_s[head]
     t_max = max_over_ranks(world, t_local)
     value = world * nodes * args.steps / t_max
+    compare = None
+    if other:
+        o_max = max_over_ranks(world, arm_s[other])
+        compare = {"schedule": other, "value": world * nodes * args.steps / o_max,
+                   "ms_per_step": 1000 * o_max / args.steps,
+                   "headline_speedup": o_max / t_max}
 
     # End to end through the public C ABI (nq_count): expansion, pinned H2D,
     # kernel, D2H of the result words.
@@ -344,13 +396,19 @@ def run_ours(args, world, rank, local):
     if not args.no_e2e:
         ecfg = nq.Config()
         ecfg.device = local
-        r = nq.count(N, k, config=ecfg)  # sizes the library's buffers for this board
+
+        def e2e_count():
+            if head == "learned":
+                return learned.count_learned(N, k, model, config=ecfg)
+            return nq.count(N, k, config=ecfg)
+
+        r = e2e_count()  # sizes the library's buffers for this board
         assert r.total == want
         barrier(world)
         walls, stats = [], []
         for i in range(args.steps):
             t0 = time.perf_counter()
-            r = nq.count(N, k, config=ecfg)
+            r = e2e_count()
             walls.append(time.perf_counter() - t0)
             if r.total != want:
                 raise SystemExit(f"e2e step {i}: count {r.total}, want {want}")
@@ -362,7 +420,9 @@ def run_ours(args, world, rank, local):
             "wall_ms_per_step": 1000 * e_max / args.steps,
             "h2d_bytes_per_step": 12 * ntasks, "d2h_bytes_per_step": 24,
             "breakdown_ms": {key: statistics.mean(s[key] for s in stats)
-                             for key in ("expand_ms", "h2d_ms", "kernel_ms", "d2h_ms", "total_ms")},
+                             for key in ("expand_ms", "h2d_ms", "schedule_ms", "kernel_ms", "d2h_ms", "total_ms")},
+            "api": "n_queens_b200.learned.count_learned (nq_count_learned)" if head == "learned"
+                   else "n_queens_b200.count (nq_count)",
         }
 
     peak_clock = None
@@ -373,12 +433,14 @@ def run_ours(args, world, rank, local):
     peak_src = "MEASURED_PEAKS.json sm_max_mhz"
     if not peak_clock:
         peak_clock, peak_src = clocks.get("sm_max_mhz") or 1965.0, "sampled clocks.max.sm"
-    achieved = (nodes * args.steps / t_local) * I_ALG / 32 / 1e9
+    achieved = (nodes * args.steps / dfs_s) * I_ALG / 32 / 1e9
     peak = sms * 4 * peak_clock * 1e6 / 1e9
     roof = {
         "bound": "int-issue", "achieved": achieved, "peak": peak, "unit": "Gwarp-inst/s", "frac": achieved / peak,
         "traffic": traffic_from_profile(f"dfs_kernel_n{N}k{k}.md"),
-        "note": (f"achieved = DFS nodes/s x {I_ALG} issue slots / 32 lanes; peak = {sms} SMs x 4 schedulers x "
+        "kernel_ms_per_launch": 1000 * dfs_s / args.steps,
+        "note": (f"achieved = DFS nodes/s of the DFS kernel alone x {I_ALG} issue slots / 32 lanes; "
+                 f"peak = {sms} SMs x 4 schedulers x "
                  f"{peak_clock:.0f} MHz ({peak_src}); traffic = ncu DRAM bytes per launch"),
     }
     if clocks.get("sm_mhz"):
@@ -400,11 +462,16 @@ def run_ours(args, world, rank, local):
             "scaling": "weak", "vs_baseline": None, "dtype": "u32 masks / u64 counts",
             "data": "synthetic (the reference's own prefix tasks; deterministic)",
             "config": {"workload": f"N={N} k={k} whole-board count", "N": N, "k": k, "tasks": int(ntasks),
-                       "dfs_nodes": int(nodes), "count": int(want), "schedule": "plain dynamic fetch",
+                       "dfs_nodes": int(nodes), "count": int(want),
+                       "schedule": ("learned longest-first (MLP cost model, device predict + sort inside each step)"
+                                    if head == "learned" else "plain dynamic fetch"),
                        "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"replicas x{world}",
                        "stack_levels": levels},
             "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-            "gpu_launches": args.steps,
+            "compare": compare, "model_build": build, "schedule_ms_per_step": sched_ms,
+            # our kernels per timed step: learned = predict + bin + DFS (the radix sort between
+            # them is CUB's), plain = DFS
+            "gpu_launches": sum(args.steps * (3 if a == "learned" else 1) for a in arms),
         }
         print(json.dumps(line), flush=True)
 

@@ -53,6 +53,13 @@ typedef enum nq_status {
  * longest-first schedule from the learned cost model. */
 enum { NQ_ORDER_PLAIN = 0, NQ_ORDER_GIVEN = 1 };
 
+/* Shared-memory stack layouts.  INTERLEAVED puts slot s of lane l at
+ * s*512 + l*16 inside the warp's block: a quarter-warp always touches 128
+ * contiguous bytes, so no stack access is bank conflicted whatever the lanes'
+ * depths.  LANE_MAJOR keeps each lane's slots contiguous (conflicts depend on
+ * the depths); it exists for the autotuner's comparison. */
+enum { NQ_LAYOUT_INTERLEAVED = 0, NQ_LAYOUT_LANE_MAJOR = 1 };
+
 /* Launch parameters; zero-initialise and set what you need.  Zero means
  * "default" (the autotuned or built-in choice) for every field. */
 typedef struct nq_config {
@@ -68,7 +75,8 @@ typedef struct nq_config {
     int device;             /* CUDA device ordinal (default 0) */
     int timing;             /* non-zero: host entries record per-CTA start/end times and fill the
                                makespan / tail fields of nq_stats */
-    int reserved[5];
+    int layout;             /* NQ_LAYOUT_INTERLEAVED (default) or NQ_LAYOUT_LANE_MAJOR */
+    int reserved[4];
 } nq_config;
 
 /* Timings and sizes of one call (all optional outputs). */
@@ -174,11 +182,40 @@ int nq_count_tasks_device_noalloc(int N, const uint32_t *d_cols, const uint32_t 
                                   int64_t n, uint64_t *d_sum, const nq_config *cfg, void *stream);
 
 /* Batched independent instances of uneven N and partial boards in one
- * persistent launch.  Each instance is split into subtasks at split_rows
- * extra rows (0 = autotuned) and out[i] receives its completions (no
- * symmetry factor, as n_queens() counts them). */
+ * persistent launch (no counterpart in the reference).  out[i] receives
+ * n_queens() of instance i (src/n_queens.cpp:8-21, no symmetry factor).
+ * Identical instances, and instances equal up to their mirror image, are
+ * counted once; a mirror-symmetric board counts its left-half children twice
+ * (the reference's half-board rule, src/n_queens.cpp:74-113, applied to any
+ * symmetric board).  Every distinct board is split split_rows rows deeper
+ * (0 = 3).  nq_count_batch = nq_batch_create + nq_batch_run + destroy. */
 int nq_count_batch(const nq_instance *inst, int64_t n, int split_rows, uint64_t *out, const nq_config *cfg,
                    nq_stats *stats);
+
+/* A reusable batch plan: the subtasks are built and uploaded once, and the
+ * queue reset + count + result copy are captured in one CUDA graph that
+ * nq_batch_run replays.  A plan keeps its device buffers until destroyed and
+ * uses its device's shared library scratch, so runs on one device are
+ * serialised. */
+typedef struct nq_batch nq_batch;
+int nq_batch_create(const nq_instance *inst, int64_t n, int split_rows, const nq_config *cfg, nq_batch **out);
+int nq_batch_run(nq_batch *b, uint64_t *out, nq_stats *stats);
+int nq_batch_destroy(nq_batch *b);
+
+/* One measured configuration of the batch autotuner. */
+typedef struct nq_tune_entry {
+    int split_rows;
+    int block_threads;
+    int layout;
+    double ms; /* mean graph replay time over `repeats` runs after one warm-up */
+} nq_tune_entry;
+
+/* Sweeps split depth 3..7, CTA size 64/128/256/512 and both stack layouts on
+ * the given instances (other launch fields from `base`), replaying each
+ * plan's graph; writes up to table_cap measured entries, their number and the
+ * fastest. */
+int nq_batch_autotune(const nq_instance *inst, int64_t n, int repeats, const nq_config *base, nq_tune_entry *table,
+                      int table_cap, int *n_entries, nq_tune_entry *best);
 
 /* ---- Learned subtree-cost scheduler (no counterpart in the reference) ----
  *
@@ -218,7 +255,9 @@ int nq_mlp_train(nq_mlp *m, const uint8_t *task_n, const uint32_t *cols, const u
 /* Longest-first order of device-resident tasks: d_order (n u32) receives the
  * task indices sorted by predicted cost, descending, in bins of 1/8 log2 unit
  * and stable inside a bin; d_pred (optional, n floats) the predictions.
- * Stream-ordered on `stream`. */
+ * Stream-ordered on `stream` (a cudaStream_t; NULL = legacy default stream).
+ * The model's prediction scratch is in use until that work completes: call no
+ * other entry of the same model before it has. */
 int nq_schedule_device(nq_mlp *m, int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd,
                        int64_t n, uint32_t *d_order, float *d_pred, void *stream);
 /* nq_count with the queue ordered by the model: expand, upload, schedule on

@@ -66,7 +66,8 @@ class Config(ctypes.Structure):
         ("time_limit_ms", ctypes.c_uint32),
         ("device", ctypes.c_int),
         ("timing", ctypes.c_int),
-        ("reserved", ctypes.c_int * 5),
+        ("layout", ctypes.c_int),
+        ("reserved", ctypes.c_int * 4),
     ]
 
 
@@ -94,6 +95,16 @@ class Stats(ctypes.Structure):
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class TuneEntry(ctypes.Structure):
+    """Mirror of ``nq_tune_entry``."""
+
+    _fields_ = [("split_rows", ctypes.c_int), ("block_threads", ctypes.c_int), ("layout", ctypes.c_int),
+                ("ms", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Instance(ctypes.Structure):
@@ -135,6 +146,17 @@ def _load() -> ctypes.CDLL:
     L.nq_count_tasks_device_noalloc.restype = ctypes.c_int
     L.nq_count_tasks_device_noalloc.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                 ctypes.c_int64, ctypes.c_void_p, _cfgp, ctypes.c_void_p]
+    L.nq_batch_create.restype = ctypes.c_int
+    L.nq_batch_create.argtypes = [ctypes.POINTER(Instance), ctypes.c_int64, ctypes.c_int, _cfgp,
+                                  ctypes.POINTER(ctypes.c_void_p)]
+    L.nq_batch_run.restype = ctypes.c_int
+    L.nq_batch_run.argtypes = [ctypes.c_void_p, _u64p, _stp]
+    L.nq_batch_destroy.restype = ctypes.c_int
+    L.nq_batch_destroy.argtypes = [ctypes.c_void_p]
+    L.nq_batch_autotune.restype = ctypes.c_int
+    L.nq_batch_autotune.argtypes = [ctypes.POINTER(Instance), ctypes.c_int64, ctypes.c_int, _cfgp,
+                                    ctypes.POINTER(TuneEntry), ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(TuneEntry)]
     L.nq_count_batch.restype = ctypes.c_int
     L.nq_count_batch.argtypes = [ctypes.POINTER(Instance), ctypes.c_int64, ctypes.c_int, _u64p, _cfgp, _stp]
     return L
@@ -145,6 +167,7 @@ lib = _load()
 # Every symbol the C header declares (checked by the CPU test suite).
 EXPORTS = ("nq_abi_version", "nq_status_string", "nq_last_error", "nq_device_count", "nq_expand", "nq_count",
            "nq_count_tasks", "nq_count_tasks_device", "nq_count_tasks_device_noalloc", "nq_count_batch",
+           "nq_batch_create", "nq_batch_run", "nq_batch_destroy", "nq_batch_autotune",
            "nq_mlp_num_params", "nq_mlp_create", "nq_mlp_destroy", "nq_mlp_get_params", "nq_mlp_set_params",
            "nq_mlp_predict", "nq_mlp_grad", "nq_mlp_train", "nq_schedule_device", "nq_count_learned")
 
@@ -278,6 +301,51 @@ def count_batch(instances, split_rows: int = 0, config=None, return_stats: bool 
     rc = lib.nq_count_batch(arr, n, split_rows, _p(out, _u64p), _cfg(config), ctypes.byref(st))
     _check(rc, "nq_count_batch")
     return (out, st.as_dict()) if return_stats else out
+
+
+def _instances(instances):
+    n = len(instances)
+    arr = (Instance * max(n, 1))()
+    for i, (N, c, l, r) in enumerate(instances):
+        arr[i] = Instance(int(N), int(c) & 0xFFFFFFFF, int(l) & 0xFFFFFFFF, int(r) & 0xFFFFFFFF)
+    return arr, n
+
+
+class BatchPlan:
+    """A reusable, graph-captured batch (``nq_batch_create`` / ``nq_batch_run``)."""
+
+    def __init__(self, instances, split_rows: int = 0, config=None):
+        arr, self.n = _instances(instances)
+        self._h = ctypes.c_void_p()
+        _check(lib.nq_batch_create(arr, self.n, split_rows, _cfg(config), ctypes.byref(self._h)), "nq_batch_create")
+
+    def run(self, return_stats: bool = False):
+        out = np.zeros(self.n, np.uint64)
+        st = Stats()
+        _check(lib.nq_batch_run(self._h, _p(out, _u64p), ctypes.byref(st)), "nq_batch_run")
+        return (out, st.as_dict()) if return_stats else out
+
+    def close(self):
+        if self._h:
+            lib.nq_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune_batch(instances, repeats: int = 2, config=None):
+    """Sweeps split depth, CTA size and stack layout; returns (best, table)."""
+    arr, n = _instances(instances)
+    table = (TuneEntry * 64)()
+    cnt = ctypes.c_int(0)
+    best = TuneEntry()
+    _check(lib.nq_batch_autotune(arr, n, repeats, _cfg(config), table, 64, ctypes.byref(cnt), ctypes.byref(best)),
+           "nq_batch_autotune")
+    return best.as_dict(), [table[i].as_dict() for i in range(min(cnt.value, 64))]
 
 
 def n_queens(N: int, cur: int, left: int, right: int) -> int:

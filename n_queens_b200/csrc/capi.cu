@@ -20,6 +20,7 @@
 #include <functional>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "dfs_kernel.cuh"
@@ -188,7 +189,7 @@ int lock_device(int dev, Ctx *&out) {
 }
 
 struct Launch {
-    int threads = 0, levels = 0, smem = 0, grid = 0, inner = 0, steal = 1;
+    int threads = 0, levels = 0, smem = 0, grid = 0, inner = 0, steal = 1, layout = 0;
 };
 
 // Chooses the persistent grid: CTA size, stack slots per lane and as many
@@ -225,6 +226,7 @@ int plan_launch(Ctx &c, const nq_config *cfg, int levels_needed, bool per_owner,
     L.grid = c.sms * per_sm;
     L.inner = (cfg && cfg->inner_steps > 0) ? ((cfg->inner_steps + 3) & ~3) : kDefaultInner;
     L.steal = (cfg && cfg->steal < 0) ? 0 : 1;
+    L.layout = (cfg && cfg->layout == NQ_LAYOUT_LANE_MAJOR) ? 1 : 0;
     return NQ_OK;
 }
 
@@ -241,6 +243,7 @@ int enqueue_dfs(Ctx &c, DfsParams p, const Launch &L, bool per_owner, bool nodes
     p.levels = L.levels;
     p.inner = L.inner;
     p.steal = L.steal;
+    p.layout = L.layout;
     NQ_CUDA(cudaMemsetAsync(p.ctl, 0, kCtlWords * sizeof(unsigned long long), s));
     if (p.cta_times) NQ_CUDA(cudaMemsetAsync(p.cta_times, 0, 2 * (size_t)L.grid * sizeof(unsigned long long), s));
     pick_kernel(per_owner, nodes)<<<L.grid, L.threads, L.smem, s>>>(p);
@@ -388,6 +391,213 @@ int count_resident(Ctx &c, int N, const uint32_t *d_cols, const uint32_t *d_ld, 
     return status_from_bits(res[2]);
 }
 
+
+constexpr int kDefaultSplit = 3;
+
+}  // namespace
+}  // namespace nqb
+
+// A batch plan: the deduplicated, split and uploaded subtasks of a set of
+// partial boards, and a CUDA graph that resets the queue, counts and copies
+// the results back.
+struct nq_batch {
+    int device = 0;
+    int64_t n_inst = 0, n_unique = 0, m_tasks = 0;
+    std::vector<int64_t> inst_to_u;
+    void *d_buf = nullptr;                 // tasks (cols | ld | rd | owner u32, task_n u8) + results
+    unsigned long long *h_res = nullptr;   // pinned: [sum, nodes, status, 2 words per unique board]
+    unsigned long long *d_out = nullptr;   // 2 words per unique board: weight-1 and weight-2 sums
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    nqb::Launch L;
+    int levels = 0;
+};
+
+namespace nqb {
+namespace {
+
+// Reverses the low N bits (column j -> N-1-j).
+uint32_t rev_bits(uint32_t x, int N) {
+    uint32_t y = 0;
+    for (int j = 0; j < N; ++j)
+        if (x >> j & 1u) y |= 1u << (N - 1 - j);
+    return y;
+}
+
+struct Board {
+    int N;
+    uint32_t c, l, r;
+    bool operator==(const Board &o) const { return N == o.N && c == o.c && l == o.l && r == o.r; }
+};
+struct BoardHash {
+    size_t operator()(const Board &b) const {
+        uint64_t h = (uint64_t)b.N * 0x9E3779B97F4A7C15ull;
+        h ^= (uint64_t)b.c + 0x632BE59BD9B4E019ull + (h << 6) + (h >> 2);
+        h ^= (uint64_t)b.l + 0x8CB92BA72F3D8DD7ull + (h << 6) + (h >> 2);
+        h ^= (uint64_t)b.r + 0xAEF17502108EF2D9ull + (h << 6) + (h >> 2);
+        return (size_t)h;
+    }
+};
+
+// The left-right mirror of a board has the same completion count.  It is
+// used only for boards whose column and right-diagonal masks lie on the
+// board (then no attack outside the board can shift back onto it, and the
+// left-diagonal bits beyond the board, which only move further out, can be
+// dropped).
+bool mirror_safe(const Board &b) {
+    const uint32_t last = (b.N >= 32) ? 0xffffffffu : ((1u << b.N) - 1u);
+    return b.N < 32 && !(b.c & ~last) && !(b.r & ~last) && b.c != last;
+}
+
+Board mirror(const Board &b) {
+    const uint32_t last = (1u << b.N) - 1u;
+    return Board{b.N, rev_bits(b.c, b.N), rev_bits(b.r & last, b.N), rev_bits(b.l & last, b.N)};
+}
+
+bool board_less(const Board &a, const Board &b) {
+    if (a.c != b.c) return a.c < b.c;
+    if (a.l != b.l) return a.l < b.l;
+    return a.r < b.r;
+}
+
+// Splits board b `rows` rows deeper into (subtask, weight) pairs whose
+// weighted counts add up to b's count.  A mirror-symmetric board keeps only
+// its left-half children at weight 2 and recurses into the middle column's
+// child (itself symmetric) -- the reference's half-board rule
+// (src/n_queens.cpp:74-113) applied to any symmetric board.
+void split_board(const Board &b, int rows, bool symmetric, std::vector<uint32_t> &tc, std::vector<uint32_t> &tl,
+                 std::vector<uint32_t> &tr, std::vector<uint8_t> &tw) {
+    if (!symmetric || rows <= 0) {
+        expand_board(b.N, b.c, b.l, b.r, rows, tc, tl, tr);
+        tw.resize(tc.size(), 1);
+        return;
+    }
+    const uint32_t last = (1u << b.N) - 1u;
+    uint32_t avail = last & ~(b.c | b.l | b.r);
+    while (avail) {
+        const uint32_t p = avail & (0u - avail);
+        avail ^= p;
+        const uint32_t q = rev_bits(p, b.N);
+        if (q < p) continue;  // right half: the mirror of a left-half child
+        const Board ch{b.N, b.c | p, (b.l | p) << 1, (uint32_t)((int32_t)(b.r | p) >> 1)};
+        if (q == p) {
+            split_board(ch, rows - 1, ch.c != last, tc, tl, tr, tw);
+        } else {
+            expand_board(ch.N, ch.c, ch.l, ch.r, rows - 1, tc, tl, tr);
+            tw.resize(tc.size(), 2);
+        }
+    }
+}
+
+void destroy_batch(nq_batch &b) {
+    if (b.exec) cudaGraphExecDestroy(b.exec);
+    if (b.graph) cudaGraphDestroy(b.graph);
+    if (b.d_buf) cudaFree(b.d_buf);
+    if (b.h_res) cudaFreeHost(b.h_res);
+    b.exec = nullptr;
+    b.graph = nullptr;
+    b.d_buf = nullptr;
+    b.h_res = nullptr;
+}
+
+int build_batch(Ctx &c, const nq_instance *inst, int64_t n, int split, const nq_config *cfg, nq_batch &B) {
+    B.device = device_of(cfg);
+    B.n_inst = n;
+    B.inst_to_u.resize((size_t)n);
+    // 1. exact dedup: identical boards, and boards equal up to mirror image
+    std::unordered_map<Board, int64_t, BoardHash> index;
+    std::vector<Board> uniq;
+    for (int64_t i = 0; i < n; ++i) {
+        Board b{inst[i].N, inst[i].cols, inst[i].ld, inst[i].rd};
+        if (mirror_safe(b)) {
+            const uint32_t last = (1u << b.N) - 1u;
+            b.l &= last;  // bits beyond the board never return
+            const Board m = mirror(b);
+            if (board_less(m, b)) b = m;
+        }
+        auto it = index.find(b);
+        if (it == index.end()) {
+            it = index.emplace(b, (int64_t)uniq.size()).first;
+            uniq.push_back(b);
+        }
+        B.inst_to_u[i] = it->second;
+    }
+    B.n_unique = (int64_t)uniq.size();
+    // 2. split every distinct board; owner = 2u + (weight == 2)
+    std::vector<uint32_t> tc, tl, tr, own;
+    std::vector<uint8_t> tw, tn;
+    int need = 1;
+    for (int64_t u = 0; u < B.n_unique; ++u) {
+        const Board &b = uniq[u];
+        const bool sym = mirror_safe(b) && mirror(b) == b;
+        const size_t before = tc.size();
+        split_board(b, split, sym, tc, tl, tr, tw);
+        const uint32_t last = (b.N >= 32) ? 0xffffffffu : ((1u << b.N) - 1u);
+        for (size_t k = before; k < tc.size(); ++k) {
+            own.push_back((uint32_t)(2 * u + (tw[k] == 2 ? 1 : 0)));
+            tn.push_back((uint8_t)b.N);
+            if (!(tc[k] & ~last) && tc[k] != last) need = std::max(need, b.N - 1 - __builtin_popcount(tc[k]));
+        }
+    }
+    const int64_t m = (int64_t)tc.size();
+    B.m_tasks = m;
+    B.levels = need;
+    int rc = plan_launch(c, cfg, need, true, false, B.L);
+    if (rc) return rc;
+    // 3. device buffer: tasks, owners, sizes, per-owner sums
+    const size_t task_bytes = ((size_t)m * 17 + 255) & ~(size_t)255;
+    const size_t out_bytes = (size_t)B.n_unique * 2 * 8;
+    NQ_CUDA(cudaMalloc(&B.d_buf, task_bytes + out_bytes + 256));
+    NQ_CUDA(cudaHostAlloc((void **)&B.h_res, (3 + 2 * (size_t)B.n_unique) * 8, cudaHostAllocDefault));
+    uint32_t *d = (uint32_t *)B.d_buf;
+    B.d_out = (unsigned long long *)((char *)B.d_buf + task_bytes);
+    if (m) {
+        NQ_CUDA(cudaMemcpyAsync(d, tc.data(), (size_t)m * 4, cudaMemcpyHostToDevice, c.stream));
+        NQ_CUDA(cudaMemcpyAsync(d + m, tl.data(), (size_t)m * 4, cudaMemcpyHostToDevice, c.stream));
+        NQ_CUDA(cudaMemcpyAsync(d + 2 * m, tr.data(), (size_t)m * 4, cudaMemcpyHostToDevice, c.stream));
+        NQ_CUDA(cudaMemcpyAsync(d + 3 * m, own.data(), (size_t)m * 4, cudaMemcpyHostToDevice, c.stream));
+        NQ_CUDA(cudaMemcpyAsync(d + 4 * m, tn.data(), (size_t)m, cudaMemcpyHostToDevice, c.stream));
+    }
+    NQ_CUDA(cudaStreamSynchronize(c.stream));
+    DfsParams p = base_params(c, 0, m, cfg);
+    p.cols = d;
+    p.ld = d + m;
+    p.rd = d + 2 * m;
+    p.owner_of = d + 3 * m;
+    p.task_n = (const uint8_t *)(d + 4 * m);
+    p.out_cnt = B.d_out;
+    p.cta_times = nullptr;
+    // 4. one graph: reset, count, copy back (result words and per-owner sums)
+    NQ_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaMemsetAsync(B.d_out, 0, out_bytes, c.stream);
+    int krc = NQ_OK;
+    if (e == cudaSuccess) krc = enqueue_dfs(c, p, B.L, true, false, c.stream);
+    if (e == cudaSuccess && krc == NQ_OK)
+        e = cudaMemcpyAsync(B.h_res, c.d_ctl + kWordSum, 3 * 8, cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess && krc == NQ_OK)
+        e = cudaMemcpyAsync(B.h_res + 3, B.d_out, out_bytes, cudaMemcpyDeviceToHost, c.stream);
+    cudaError_t e2 = cudaStreamEndCapture(c.stream, &B.graph);
+    if (krc) return krc;
+    if (e != cudaSuccess) return fail_cuda(e, "batch graph capture");
+    if (e2 != cudaSuccess) return fail_cuda(e2, "cudaStreamEndCapture");
+    NQ_CUDA(cudaGraphInstantiate(&B.exec, B.graph, 0));
+    return NQ_OK;
+}
+
+int run_batch(Ctx &c, nq_batch &B, nq_stats *st) {
+    NQ_CUDA(cudaEventRecord(c.ev[1], c.stream));
+    NQ_CUDA(cudaGraphLaunch(B.exec, c.stream));
+    NQ_CUDA(cudaEventRecord(c.ev[2], c.stream));
+    NQ_CUDA(cudaStreamSynchronize(c.stream));
+    if (st) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c.ev[1], c.ev[2]);
+        st->kernel_ms = ms;
+        st->tasks = B.m_tasks;
+        fill_stats_launch(st, B.L);
+    }
+    return NQ_OK;
+}
 }  // namespace
 
 void set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
@@ -657,12 +867,11 @@ int nq_count_tasks_device(int N, const uint32_t *d_cols, const uint32_t *d_ld, c
     return enqueue_dfs(c, p, L, per_owner, want_nodes, s);
 }
 
-int nq_count_batch(const nq_instance *inst, int64_t n, int split_rows, uint64_t *out, const nq_config *cfg,
-                   nq_stats *stats) {
-    const double t0 = now_ms();
-    if (stats) memset(stats, 0, sizeof(*stats));
-    if (n < 0 || (n > 0 && (!inst || !out)) || split_rows < 0 || split_rows > 8) return NQ_ERR_ARG;
-    if (n > 0xffffffffll) return NQ_ERR_ARG;
+int nq_batch_create(const nq_instance *inst, int64_t n, int split_rows, const nq_config *cfg, nq_batch **out) {
+    if (!out) return NQ_ERR_ARG;
+    *out = nullptr;
+    if (n < 0 || (n > 0 && !inst) || split_rows < 0 || split_rows > 8) return NQ_ERR_ARG;
+    if (n > 0x7fffffffll) return NQ_ERR_ARG;
     for (int64_t i = 0; i < n; ++i)
         if (inst[i].N < 1 || inst[i].N > NQ_MAX_N) return NQ_ERR_ARG;
     Ctx *cp = nullptr;
@@ -672,77 +881,101 @@ int nq_count_batch(const nq_instance *inst, int64_t n, int split_rows, uint64_t 
     std::lock_guard<std::mutex> lock(c.mu);
     rc = ensure_ready(c, device_of(cfg));
     if (rc) return rc;
-    if (n == 0) return NQ_OK;
-    const int split = split_rows ? split_rows : 3;
+    nq_batch *b = new nq_batch();
+    rc = build_batch(c, inst, n, split_rows ? split_rows : kDefaultSplit, cfg, *b);
+    if (rc) {
+        destroy_batch(*b);
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return NQ_OK;
+}
 
-    // Split every instance into subtasks; a subtask remembers its instance
-    // (owner) and board size.
-    const double te = now_ms();
-    std::vector<uint32_t> tc, tl, tr, own;
-    std::vector<uint8_t> tn;
-    int need = 1;
-    for (int64_t i = 0; i < n; ++i) {
-        const int N = inst[i].N;
-        const size_t before = tc.size();
-        expand_board(N, inst[i].cols, inst[i].ld, inst[i].rd, split, tc, tl, tr);
-        const uint32_t last = (N >= 32) ? 0xffffffffu : ((1u << N) - 1u);
-        for (size_t k = before; k < tc.size(); ++k) {
-            own.push_back((uint32_t)i);
-            tn.push_back((uint8_t)N);
-            if (!(tc[k] & ~last) && tc[k] != last) need = std::max(need, N - 1 - __builtin_popcount(tc[k]));
-        }
-    }
-    const int64_t m = (int64_t)tc.size();
-    if (stats) {
-        stats->expand_ms = now_ms() - te;
-        stats->tasks = m;
-    }
-    // tasks: cols | ld | rd | owner (u32 each), then task_n (u8)
-    rc = c.tasks.grow((size_t)m * 17 + 256);
+int nq_batch_run(nq_batch *b, uint64_t *out, nq_stats *stats) {
+    if (!b || (b->n_inst > 0 && !out)) return NQ_ERR_ARG;
+    const double t0 = now_ms();
+    if (stats) memset(stats, 0, sizeof(*stats));
+    Ctx &c = g_ctx[b->device];
+    std::lock_guard<std::mutex> lock(c.mu);
+    NQ_CUDA(cudaSetDevice(b->device));
+    int rc = run_batch(c, *b, stats);
     if (rc) return rc;
-    uint32_t *d = (uint32_t *)c.tasks.p;
-    NQ_CUDA(cudaEventRecord(c.ev[0], c.stream));
-    if (m) {
-        NQ_CUDA(cudaMemcpyAsync(d, tc.data(), (size_t)m * 4, cudaMemcpyHostToDevice, c.stream));
-        NQ_CUDA(cudaMemcpyAsync(d + m, tl.data(), (size_t)m * 4, cudaMemcpyHostToDevice, c.stream));
-        NQ_CUDA(cudaMemcpyAsync(d + 2 * m, tr.data(), (size_t)m * 4, cudaMemcpyHostToDevice, c.stream));
-        NQ_CUDA(cudaMemcpyAsync(d + 3 * m, own.data(), (size_t)m * 4, cudaMemcpyHostToDevice, c.stream));
-        NQ_CUDA(cudaMemcpyAsync(d + 4 * m, tn.data(), (size_t)m, cudaMemcpyHostToDevice, c.stream));
+    for (int64_t i = 0; i < b->n_inst; ++i) {
+        const int64_t u = b->inst_to_u[i];
+        out[i] = b->h_res[3 + 2 * u] + 2 * b->h_res[3 + 2 * u + 1];
     }
-    Launch L;
-    rc = plan_launch(c, cfg, need, true, false, L);
-    if (rc) return rc;
-    fill_stats_launch(stats, L);
-    rc = c.aux.grow((size_t)n * 8);
-    if (rc) return rc;
-    DfsParams p = base_params(c, 0, m, cfg);
-    p.cols = d;
-    p.ld = d + m;
-    p.rd = d + 2 * m;
-    p.owner_of = d + 3 * m;
-    p.task_n = (const uint8_t *)(d + 4 * m);
-    p.out_cnt = (unsigned long long *)c.aux.p;
-    NQ_CUDA(cudaMemsetAsync(p.out_cnt, 0, (size_t)n * 8, c.stream));
-    NQ_CUDA(cudaEventRecord(c.ev[1], c.stream));
-    rc = enqueue_dfs(c, p, L, true, false, c.stream);
-    if (rc) return rc;
-    NQ_CUDA(cudaEventRecord(c.ev[2], c.stream));
-    unsigned long long res[3] = {0, 0, 0};
-    NQ_CUDA(cudaMemcpyAsync(res, c.d_ctl + kWordSum, sizeof(res), cudaMemcpyDeviceToHost, c.stream));
-    NQ_CUDA(cudaMemcpyAsync(out, p.out_cnt, (size_t)n * 8, cudaMemcpyDeviceToHost, c.stream));
-    NQ_CUDA(cudaEventRecord(c.ev[3], c.stream));
-    NQ_CUDA(cudaStreamSynchronize(c.stream));
-    if (stats) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]);
-        stats->h2d_ms = ms;
-        cudaEventElapsedTime(&ms, c.ev[1], c.ev[2]);
-        stats->kernel_ms = ms;
-        cudaEventElapsedTime(&ms, c.ev[2], c.ev[3]);
-        stats->d2h_ms = ms;
-        stats->total_ms = now_ms() - t0;
+    if (stats) stats->total_ms = now_ms() - t0;
+    return status_from_bits(b->h_res[2]);
+}
+
+int nq_batch_destroy(nq_batch *b) {
+    if (!b) return NQ_OK;
+    {
+        Ctx &c = g_ctx[b->device];
+        std::lock_guard<std::mutex> lock(c.mu);
+        cudaSetDevice(b->device);
+        destroy_batch(*b);
     }
-    return status_from_bits(res[2]);
+    delete b;
+    return NQ_OK;
+}
+
+int nq_batch_autotune(const nq_instance *inst, int64_t n, int repeats, const nq_config *base, nq_tune_entry *table,
+                      int table_cap, int *n_entries, nq_tune_entry *best) {
+    if (!inst || n <= 0 || repeats < 1 || !best || table_cap < 0 || (table_cap > 0 && !table)) return NQ_ERR_ARG;
+    static const int kSplits[] = {3, 4, 5, 6, 7};
+    static const int kThreads[] = {64, 128, 256, 512};
+    static const int kLayouts[] = {NQ_LAYOUT_INTERLEAVED, NQ_LAYOUT_LANE_MAJOR};
+    nq_config cfg;
+    if (base)
+        cfg = *base;
+    else
+        memset(&cfg, 0, sizeof(cfg));
+    int count = 0;
+    best->ms = -1.0;
+    for (int split : kSplits)
+        for (int threads : kThreads)
+            for (int layout : kLayouts) {
+                cfg.block_threads = threads;
+                cfg.layout = layout;
+                nq_batch *b = nullptr;
+                int rc = nq_batch_create(inst, n, split, &cfg, &b);
+                if (rc == NQ_ERR_DEPTH) continue;  // this CTA size cannot hold the stacks
+                if (rc) return rc;
+                std::vector<uint64_t> outv((size_t)n);
+                nq_stats st;
+                rc = nq_batch_run(b, outv.data(), &st);  // warm-up
+                double sum_ms = 0;
+                for (int r = 0; r < repeats && rc == NQ_OK; ++r) {
+                    rc = nq_batch_run(b, outv.data(), &st);
+                    sum_ms += st.kernel_ms;
+                }
+                nq_batch_destroy(b);
+                if (rc) return rc;
+                nq_tune_entry e;
+                e.split_rows = split;
+                e.block_threads = threads;
+                e.layout = layout;
+                e.ms = sum_ms / repeats;
+                if (count < table_cap) table[count] = e;
+                ++count;
+                if (best->ms < 0 || e.ms < best->ms) *best = e;
+            }
+    if (n_entries) *n_entries = count;
+    return best->ms < 0 ? NQ_ERR_ARG : NQ_OK;
+}
+
+int nq_count_batch(const nq_instance *inst, int64_t n, int split_rows, uint64_t *out, const nq_config *cfg,
+                   nq_stats *stats) {
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (n == 0) return (n < 0 || split_rows < 0 || split_rows > 8) ? NQ_ERR_ARG : NQ_OK;
+    nq_batch *b = nullptr;
+    int rc = nq_batch_create(inst, n, split_rows, cfg, &b);
+    if (rc) return rc;
+    rc = nq_batch_run(b, out, stats);
+    nq_batch_destroy(b);
+    return rc;
 }
 
 }  // extern "C"

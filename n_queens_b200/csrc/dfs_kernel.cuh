@@ -76,6 +76,7 @@ struct DfsParams {
     unsigned long long *status_out;  // kStat* bits of this launch (device word)
     uint32_t k_one, k_two, k_mone;   // 1, 2, -1 (see dfs_step)
     unsigned long long *cta_times;   // optional [2*gridDim.x]: %globaltimer at CTA start and end
+    int layout;                      // stack layout: 0 interleaved (default), 1 lane-major
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -106,9 +107,10 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
 // Right shift is arithmetic, as in the reference's `int` arithmetic.
 //
 // Operands: %0 cols, %1 ld, %2 rd, %3 avail, %4 sp, %5 cnt, %6 placements
-// (node statistics), %7 bot, %8 = 1, %9 = 2, %10 = -1.  The three constants
-// arrive as kernel parameters, so the compiler cannot fold the multiply-adds
-// below back into ALU adds/moves.
+// (node statistics), %7 bot, %8 = 1, %9 = 2, %10 = -1, %11 the slot stride
+// (512 B interleaved, 16 B lane-major).  The constants arrive as kernel
+// parameters, so the compiler cannot fold the multiply-adds below back into
+// ALU adds/moves.
 //
 // VAR 0 issues everything as logic/ALU operations.  VAR 1 moves the adds,
 // the left shift and the four register moves to multiply-add form (the FMA
@@ -154,14 +156,14 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "setp.ne.and.u32 pd, na, 0, pb;\n\t"                                              \
     "setp.ne.and.u32 pp, %3, 0, pd;\n\t"                                              \
     "@pp st.shared.v4.u32 [%4], {%0, %1, %2, %3};\n\t"                                \
-    "@pp add.u32 %4, %4, 512;\n\t"                                                    \
+    "@pp add.u32 %4, %4, %11;\n\t"                                                    \
     "@pd mov.b32 %0, nc;\n\t"                                                         \
     "@pd mov.b32 %1, nl;\n\t"                                                         \
     "@pd mov.b32 %2, nr;\n\t"                                                         \
     "@pd mov.b32 %3, na;\n\t"                                                         \
     "setp.eq.u32 pq, %3, 0;\n\t"                                                      \
     "setp.ne.and.u32 pq, %4, %7, pq;\n\t"                                             \
-    "@pq sub.u32 %4, %4, 512;\n\t"                                                    \
+    "@pq sub.u32 %4, %4, %11;\n\t"                                                    \
     "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"                                \
     "}\n\t"
 
@@ -169,19 +171,19 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "setp.ne.and.u32 pd, na, 0, pb;\n\t"                                              \
     "setp.ne.and.u32 pp, %3, 0, pd;\n\t"                                              \
     "@pp st.shared.v4.u32 [%4], {%0, %1, %2, %3};\n\t"                                \
-    "@pp mad.lo.s32 %4, %8, 512, %4;\n\t"                                             \
+    "@pp mad.lo.s32 %4, %8, %11, %4;\n\t"                                             \
     "@pd mul.lo.s32 %0, nc, %8;\n\t"                                                  \
     "@pd mul.lo.s32 %1, nl, %8;\n\t"                                                  \
     "@pd mul.lo.s32 %2, nr, %8;\n\t"                                                  \
     "@pd mul.lo.s32 %3, na, %8;\n\t"                                                  \
     "setp.eq.u32 pq, %3, 0;\n\t"                                                      \
     "setp.ne.and.u32 pq, %4, %7, pq;\n\t"                                             \
-    "@pq mad.lo.s32 %4, %8, -512, %4;\n\t"                                            \
+    "@pq mad.lo.s32 %4, %10, %11, %4;\n\t"                                            \
     "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"                                \
     "}\n\t"
 
 struct StepConsts {
-    uint32_t one, two, mone;
+    uint32_t one, two, mone, stride;  // stride: bytes between a lane's consecutive stack slots
 };
 
 template <bool NODES, int VAR>
@@ -189,7 +191,7 @@ __device__ __forceinline__ void dfs_step(uint32_t &cols, uint32_t &ld, uint32_t 
                                          uint32_t &cnt, uint32_t &it, uint32_t bot, const StepConsts &k) {
 #define NQB_STEP_OPERANDS                                                                         \
     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)                   \
-    : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone)                                               \
+    : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride)                                \
     : "memory"
     if (VAR == 0) {
         if (NODES)
@@ -243,10 +245,16 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t smem_base = (uint32_t)__cvta_generic_to_shared(smem_raw);
-    const uint32_t my_base = smem_base + warp * (uint32_t)p.levels * kSlotBytes + lane * 16u;
+    // Stack layout 0 (interleaved): slot s of lane l at warp_base + s*512 + l*16,
+    // conflict-free for every mix of depths.  Layout 1 (lane-major): each
+    // lane's slots contiguous, lane_base + s*16 (kept for the autotuner).
+    const uint32_t stride = p.layout == 1 ? 16u : kSlotBytes;
+    const uint32_t my_base = p.layout == 1
+                                 ? smem_base + (warp * 32u + lane) * (uint32_t)p.levels * 16u
+                                 : smem_base + warp * (uint32_t)p.levels * kSlotBytes + lane * 16u;
 
     if (p.cta_times && threadIdx.x == 0) p.cta_times[2 * blockIdx.x] = globaltimer_ns();
-    const StepConsts kc{p.k_one, p.k_two, p.k_mone};
+    const StepConsts kc{p.k_one, p.k_two, p.k_mone, stride};
     uint32_t cols = 0, ld = 0, rd = 0, avail = 0;
     uint32_t sp = my_base, bot = my_base;
     uint32_t cnt = 0, it = 0;
@@ -347,7 +355,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                             owner = src_owner;
                         }
                         __syncwarp();
-                        if (sp != bot && __popc(rich & lanemask_lt()) < npair) bot += kSlotBytes;
+                        if (sp != bot && __popc(rich & lanemask_lt()) < npair) bot += stride;
                         __syncwarp();
                     } else {
                         // Nobody can donate right now: run a full trip

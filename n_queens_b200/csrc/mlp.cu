@@ -711,7 +711,7 @@ int nq_schedule_device(nq_mlp *m, int N, const uint32_t *d_cols, const uint32_t 
         return NQ_ERR_ARG;
     if (n == 0) return NQ_OK;
     std::lock_guard<std::mutex> lock(m->mu);
-    cudaStream_t s = stream ? (cudaStream_t)stream : m->stream;
+    cudaStream_t s = (cudaStream_t)stream;  // NULL: the legacy default stream, as in every device entry
     // scratch: pred f32 | key u16 | key_out u16 | idx u32
     const size_t need = (size_t)n * (4 + 2 + 2 + 4) + 1024;
     rc = grow(m->data, m->data_cap, need);

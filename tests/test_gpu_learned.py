@@ -132,3 +132,27 @@ def test_learned_count_is_exact_and_front_loads_work(gpu, golden):
           f"oracle {share_oracle:.3f}")
     assert share_learned > share_plain + 0.15
     model.close()
+
+
+def test_device_schedule_then_count_on_one_stream(gpu, golden):
+    # Schedule and count enqueued back to back on the default stream, no
+    # synchronisation in between (the bench's learned step).
+    import torch
+    from n_queens_b200 import learned
+    N, k = 17, 6
+    m = learned.CostModel(seed=9)
+    c, l, r = oracle.expand(N, k)
+    dev = torch.device("cuda:0")
+    tc, tl, tr = (torch.from_numpy(a.view(np.int32)).to(dev) for a in (c, l, r))
+    order = torch.empty(c.size, dtype=torch.int32, device=dev)
+    out = torch.zeros(2, dtype=torch.int64, device=dev)
+    cfg = gpu.Config()
+    cfg.stack_levels = N - 1 - k
+    cfg.order_kind = gpu.NQ_ORDER_GIVEN
+    cfg.order = order.data_ptr()
+    for _ in range(2):
+        assert learned.lib.nq_schedule_device(m._m, N, tc.data_ptr(), tl.data_ptr(), tr.data_ptr(), c.size,
+                                              order.data_ptr(), None, None) == 0
+        gpu.count_tasks_device(N, tc, tl, tr, out, config=cfg)
+        assert 2 * int(out[0]) == golden("published.json")[str(N)]["total"] and int(out[1]) == 0
+    m.close()

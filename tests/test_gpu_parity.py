@@ -170,3 +170,45 @@ def test_cli_result_line(gpu):
     assert "cuda 16 queens result 14772512, calc time: [" in out
     assert "to generate 70906 subproblems!" in out
     assert "gpu [0] start job, with 70906(1.00) subproblems." in out
+
+
+def test_batch_dedup_and_symmetry(gpu):
+    # Duplicates, mirror images, empty boards (symmetric: half-board rule)
+    # and a symmetric odd board with a middle queen, all against the oracle.
+    boards = []
+    for N in range(4, 13):
+        boards.append((N, 0, 0, 0))
+        if N % 2:
+            p = 1 << (N // 2)
+            boards.append((N, p, p << 1, p >> 1))
+    base = workloads.random_boards(120, 21, 8, 13, 0, 5)
+    boards += base + base[:30]
+    boards += [(N,) + workloads.mirror_board(N, c, l, r) for (N, c, l, r) in base[30:60]]
+    want = [oracle.count_task(*b) for b in boards]
+    for cfg in (None, dict(layout=1), dict(block_threads=64)):
+        for split in (0, 1, 4, 7):
+            assert gpu.count_batch(boards, split_rows=split, config=cfg).tolist() == want, (cfg, split)
+
+
+def test_batch_plan_replays(gpu, golden):
+    g = golden("boards_small.json")
+    inst = [tuple(b) for b in g["instances"]]
+    plan = gpu.BatchPlan(inst, split_rows=4)
+    for _ in range(3):
+        out, st = plan.run(return_stats=True)
+        assert out.tolist() == g["counts"]
+        assert st["tasks"] > 0 and st["kernel_ms"] > 0
+    plan.close()
+
+
+def test_batch_autotune_sweep(gpu):
+    inst = workloads.random_boards(96, 4, 9, 13, 0, 3)
+    want = [oracle.count_task(*b) for b in inst]
+    best, table = gpu.autotune_batch(inst, repeats=1)
+    assert len(table) == 40
+    assert {e["split_rows"] for e in table} == {3, 4, 5, 6, 7}
+    assert {e["block_threads"] for e in table} == {64, 128, 256, 512}
+    assert {e["layout"] for e in table} == {0, 1}
+    assert best["ms"] == min(e["ms"] for e in table)
+    cfg = dict(block_threads=best["block_threads"], layout=best["layout"])
+    assert gpu.count_batch(inst, split_rows=best["split_rows"], config=cfg).tolist() == want
