@@ -34,7 +34,7 @@ namespace {
 constexpr int kMaxDevices = 64;
 constexpr int kMaxBlocksPerSm = 32;
 constexpr int kDefaultThreads = 256;
-constexpr int kDefaultInner = 256;
+constexpr int kDefaultInner = 1024;
 // d_ctl layout (uint64 words): control words, results, per-CTA partials.
 constexpr int kWordSum = kCtlWords + 0;
 constexpr int kWordNodes = kCtlWords + 1;
