@@ -140,6 +140,20 @@ int nq_expand(int N, int rows, uint32_t *cols, uint32_t *ld, uint32_t *rd, int64
  * raises rows to 2 (src/main.cpp:26-29) and so does this library's CLI. */
 int nq_count(int N, int rows, const nq_config *cfg, uint64_t *total, uint64_t *nodes, nq_stats *stats);
 
+/* Time-sliced, resumable whole-board count (no counterpart in the reference,
+ * whose N=26/27 runs took 2.5 and 28.4 days with no way to stop and resume,
+ * README.md:41-48).  Same total as nq_count.  If checkpoint_path exists the
+ * count resumes from it (it must be for the same N and rows).  With
+ * cfg->time_limit_ms > 0 the kernel stops after that long: every lane saves
+ * its unfinished DFS levels, and the queue cursor, the partial sum and those
+ * levels are written to checkpoint_path (atomically, via a .tmp file);
+ * *done = 0 and NQ_OK are returned.  Once the count finishes, *done = 1,
+ * *total holds it and the checkpoint file is removed.  Call again until done.
+ * Saved work is never counted twice or lost: each level is either finished
+ * (and in the partial sum) or saved with only its untried columns. */
+int nq_count_resumable(int N, int rows, const nq_config *cfg, const char *checkpoint_path, uint64_t *total,
+                       int *done, nq_stats *stats);
+
 /* Counts over a caller-built task list in host memory.  Replaces the
  * per-GPU upload / launch / download of src/n_queens_cuda.cu:156-177 with
  * the per-task semantics of n_queens() (src/n_queens.cpp:8-21).

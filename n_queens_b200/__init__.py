@@ -136,6 +136,9 @@ def _load() -> ctypes.CDLL:
     L.nq_expand.argtypes = [ctypes.c_int, ctypes.c_int, _u32p, _u32p, _u32p, ctypes.c_int64, _i64p, ctypes.c_int]
     L.nq_count.restype = ctypes.c_int
     L.nq_count.argtypes = [ctypes.c_int, ctypes.c_int, _cfgp, _u64p, _u64p, _stp]
+    L.nq_count_resumable.restype = ctypes.c_int
+    L.nq_count_resumable.argtypes = [ctypes.c_int, ctypes.c_int, _cfgp, ctypes.c_char_p, _u64p,
+                                     ctypes.POINTER(ctypes.c_int), _stp]
     L.nq_count_tasks.restype = ctypes.c_int
     L.nq_count_tasks.argtypes = [ctypes.c_int, _u32p, _u32p, _u32p, ctypes.c_int64, _u64p, _u64p, _u64p, _cfgp,
                                  _stp]
@@ -166,6 +169,7 @@ lib = _load()
 
 # Every symbol the C header declares (checked by the CPU test suite).
 EXPORTS = ("nq_abi_version", "nq_status_string", "nq_last_error", "nq_device_count", "nq_expand", "nq_count",
+           "nq_count_resumable",
            "nq_count_tasks", "nq_count_tasks_device", "nq_count_tasks_device_noalloc", "nq_count_batch",
            "nq_batch_create", "nq_batch_run", "nq_batch_destroy", "nq_batch_autotune",
            "nq_mlp_num_params", "nq_mlp_create", "nq_mlp_destroy", "nq_mlp_get_params", "nq_mlp_set_params",
@@ -240,6 +244,28 @@ def count(N: int, rows: int, config=None, nodes: bool = False) -> CountResult:
                       ctypes.byref(st))
     _check(rc, "nq_count")
     return CountResult(int(tot.value), int(nd.value) if nodes else None, st.as_dict())
+
+
+def count_resumable(N: int, rows: int, checkpoint: str, slice_ms: int = 0, config=None):
+    """One slice of a resumable whole-board count (``nq_count_resumable``).
+
+    Returns (done, total, stats); total is valid once done.  Call again with
+    the same checkpoint path until done.
+    """
+    c = Config()
+    if config is not None:
+        for k, v in (config.items() if isinstance(config, dict) else []):
+            setattr(c, k, v)
+        if isinstance(config, Config):
+            c = config
+    c.time_limit_ms = slice_ms
+    tot = ctypes.c_uint64(0)
+    done = ctypes.c_int(0)
+    st = Stats()
+    rc = lib.nq_count_resumable(N, rows, ctypes.byref(c), os.fsencode(checkpoint), ctypes.byref(tot),
+                                ctypes.byref(done), ctypes.byref(st))
+    _check(rc, "nq_count_resumable")
+    return bool(done.value), int(tot.value), st.as_dict()
 
 
 def cuda_n_queens(N: int, rows: int) -> int:

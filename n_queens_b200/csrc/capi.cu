@@ -13,9 +13,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdlib.h>
+#include <stdio.h>
 #include <string.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <chrono>
 #include <functional>
 #include <mutex>
@@ -392,6 +394,80 @@ int count_resident(Ctx &c, int N, const uint32_t *d_cols, const uint32_t *d_ld, 
 }
 
 
+
+// Checkpoint of a resumable whole-board count (little-endian file):
+//   "NQB200CK" | u32 version=1 | i32 N | i32 rows | i32 0 | i64 ntasks |
+//   i64 cursor | u64 partial (plain sum so far) | u64 slices | i64 n_cont |
+//   n_cont x 16-byte continuation entries (cols|~last, ld, rd, untried)
+struct Checkpoint {
+    int N = 0, rows = 0;
+    int64_t ntasks = 0, cursor = 0;
+    uint64_t partial = 0, slices = 0;
+    std::vector<uint4> cont;
+};
+
+const char kCkMagic[8] = {'N', 'Q', 'B', '2', '0', '0', 'C', 'K'};
+
+int read_checkpoint(const char *path, int N, int rows, Checkpoint &ck, bool &have) {
+    have = false;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return NQ_OK;  // no checkpoint yet: start from the beginning
+    char magic[8];
+    uint32_t version = 0;
+    int32_t hN = 0, hrows = 0, pad = 0;
+    int64_t n_cont = -1;
+    bool ok = std::fread(magic, 1, 8, f) == 8 && memcmp(magic, kCkMagic, 8) == 0 &&
+              std::fread(&version, 4, 1, f) == 1 && version == 1 && std::fread(&hN, 4, 1, f) == 1 &&
+              std::fread(&hrows, 4, 1, f) == 1 && std::fread(&pad, 4, 1, f) == 1 &&
+              std::fread(&ck.ntasks, 8, 1, f) == 1 && std::fread(&ck.cursor, 8, 1, f) == 1 &&
+              std::fread(&ck.partial, 8, 1, f) == 1 && std::fread(&ck.slices, 8, 1, f) == 1 &&
+              std::fread(&n_cont, 8, 1, f) == 1 && n_cont >= 0 && n_cont < (int64_t)1 << 32;
+    if (ok) {
+        ck.cont.resize((size_t)n_cont);
+        ok = n_cont == 0 || std::fread(ck.cont.data(), 16, (size_t)n_cont, f) == (size_t)n_cont;
+        char extra;
+        ok = ok && std::fread(&extra, 1, 1, f) == 0;  // nothing after the entries
+    }
+    std::fclose(f);
+    if (!ok) {
+        g_last_error = std::string("not a valid checkpoint file: ") + path;
+        return NQ_ERR_ARG;
+    }
+    if (hN != N || hrows != rows) {
+        g_last_error = "checkpoint is for N=" + std::to_string(hN) + " rows=" + std::to_string(hrows);
+        return NQ_ERR_ARG;
+    }
+    ck.N = hN;
+    ck.rows = hrows;
+    have = true;
+    return NQ_OK;
+}
+
+int write_checkpoint(const char *path, const Checkpoint &ck) {
+    const std::string tmp = std::string(path) + ".tmp";
+    FILE *f = std::fopen(tmp.c_str(), "wb");
+    if (!f) {
+        g_last_error = "cannot write " + tmp;
+        return NQ_ERR_ARG;
+    }
+    const uint32_t version = 1;
+    const int32_t hN = ck.N, hrows = ck.rows, pad = 0;
+    const int64_t n_cont = (int64_t)ck.cont.size();
+    bool ok = std::fwrite(kCkMagic, 1, 8, f) == 8 && std::fwrite(&version, 4, 1, f) == 1 &&
+              std::fwrite(&hN, 4, 1, f) == 1 && std::fwrite(&hrows, 4, 1, f) == 1 && std::fwrite(&pad, 4, 1, f) == 1 &&
+              std::fwrite(&ck.ntasks, 8, 1, f) == 1 && std::fwrite(&ck.cursor, 8, 1, f) == 1 &&
+              std::fwrite(&ck.partial, 8, 1, f) == 1 && std::fwrite(&ck.slices, 8, 1, f) == 1 &&
+              std::fwrite(&n_cont, 8, 1, f) == 1 &&
+              (n_cont == 0 || std::fwrite(ck.cont.data(), 16, (size_t)n_cont, f) == (size_t)n_cont);
+    ok = (std::fflush(f) == 0) && ok;
+    std::fclose(f);
+    if (!ok || std::rename(tmp.c_str(), path) != 0) {
+        g_last_error = "cannot write checkpoint " + std::string(path);
+        return NQ_ERR_ARG;
+    }
+    return NQ_OK;
+}
+
 constexpr int kDefaultSplit = 3;
 
 }  // namespace
@@ -713,6 +789,119 @@ int nq_count(int N, int rows, const nq_config *cfg, uint64_t *total, uint64_t *n
     if (nodes) *nodes = nd;
     if (stats) stats->total_ms = now_ms() - t0;
     return rc;
+}
+
+int nq_count_resumable(int N, int rows, const nq_config *cfg, const char *checkpoint_path, uint64_t *total,
+                       int *done, nq_stats *stats) {
+    const double t0 = now_ms();
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (N < 2 || N > NQ_MAX_N || rows < 1 || rows > N - 2 || !total || !done || !checkpoint_path) return NQ_ERR_ARG;
+    *done = 0;
+    *total = 0;
+    Checkpoint ck;
+    bool have = false;
+    int rc = read_checkpoint(checkpoint_path, N, rows, ck, have);
+    if (rc) return rc;
+    Ctx *cp = nullptr;
+    rc = lock_device(device_of(cfg), cp);
+    if (rc) return rc;
+    Ctx &c = *cp;
+    std::lock_guard<std::mutex> lock(c.mu);
+    rc = ensure_ready(c, device_of(cfg));
+    if (rc) return rc;
+    const double te = now_ms();
+    const int64_t n = expand_prefixes(N, rows, nullptr, nullptr, nullptr, 0, 0);
+    if (n < 0) return NQ_ERR_ARG;
+    if (have && (ck.ntasks != n || ck.cursor < 0 || ck.cursor > n)) {
+        g_last_error = "checkpoint does not match this board's task list";
+        return NQ_ERR_ARG;
+    }
+    const size_t ncont = have ? ck.cont.size() : 0;
+    rc = c.h_tasks.grow((size_t)std::max<int64_t>(n, 1) * 12);
+    if (rc) return rc;
+    uint32_t *h = (uint32_t *)c.h_tasks.p;
+    expand_prefixes(N, rows, h, h + n, h + 2 * n, n, 0);
+    if (stats) {
+        stats->expand_ms = now_ms() - te;
+        stats->tasks = n;
+    }
+    // tasks, then the continuation entries to resume
+    const size_t task_bytes = ((size_t)std::max<int64_t>(n, 1) * 12 + 255) & ~(size_t)255;
+    rc = c.tasks.grow(task_bytes + ncont * 16 + 256);
+    if (rc) return rc;
+    uint32_t *d = (uint32_t *)c.tasks.p;
+    uint4 *d_cont_in = (uint4 *)((char *)c.tasks.p + task_bytes);
+    NQ_CUDA(cudaEventRecord(c.ev[0], c.stream));
+    if (n) NQ_CUDA(cudaMemcpyAsync(d, h, (size_t)n * 12, cudaMemcpyHostToDevice, c.stream));
+    if (ncont)
+        NQ_CUDA(cudaMemcpyAsync(d_cont_in, ck.cont.data(), ncont * 16, cudaMemcpyHostToDevice, c.stream));
+    Launch L;
+    rc = plan_launch(c, cfg, N - 1 - rows, false, false, L);
+    if (rc) return rc;
+    fill_stats_launch(stats, L);
+    // room for every lane's unfinished levels: the current one + one per slot
+    const size_t cap = (size_t)L.grid * L.threads * (L.levels + 1);
+    rc = c.aux.grow(cap * 16);
+    if (rc) return rc;
+    DfsParams p = base_params(c, N, n, cfg);
+    p.cols = d;
+    p.ld = d + n;
+    p.rd = d + 2 * n;
+    p.cont_in = d_cont_in;
+    p.n_cont_in = (long long)ncont;
+    p.task_base = have ? ck.cursor : 0;
+    p.cont_out = (uint4 *)c.aux.p;
+    p.cont_cap = (long long)cap;
+    NQ_CUDA(cudaEventRecord(c.ev[1], c.stream));
+    rc = enqueue_dfs(c, p, L, false, false, c.stream);
+    if (rc) return rc;
+    NQ_CUDA(cudaEventRecord(c.ev[2], c.stream));
+    unsigned long long words[kWordBlocks];
+    NQ_CUDA(cudaMemcpyAsync(words, c.d_ctl, sizeof(words), cudaMemcpyDeviceToHost, c.stream));
+    NQ_CUDA(cudaStreamSynchronize(c.stream));
+    if (stats) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]);
+        stats->h2d_ms = ms;
+        cudaEventElapsedTime(&ms, c.ev[1], c.ev[2]);
+        stats->kernel_ms = ms;
+    }
+    const unsigned long long bits = words[kWordStatus];
+    if (bits & kStatContOverflow) {
+        g_last_error = "continuation buffer overflow";
+        return NQ_ERR_CUDA;
+    }
+    if (bits & kStatDepth) return status_from_bits(bits);
+    const uint64_t partial = (have ? ck.partial : 0) + words[kWordSum];
+    if (bits & kStatTimeout) {
+        // Positions taken from the queue were either finished or saved.
+        const long long qlen = (long long)ncont + n - p.task_base;
+        const long long taken = std::min<long long>((long long)words[kCtlHead], qlen);
+        Checkpoint out;
+        out.N = N;
+        out.rows = rows;
+        out.ntasks = n;
+        out.cursor = p.task_base + std::max<long long>(0, taken - (long long)ncont);
+        out.partial = partial;
+        out.slices = (have ? ck.slices : 0) + 1;
+        // Saved levels of an earlier slice that no lane picked up this time
+        // carry over unchanged, then come the levels this slice saved.
+        const size_t untaken = (size_t)std::max<long long>(0, (long long)ncont - taken);
+        const size_t fresh = (size_t)words[kCtlCont];
+        out.cont.resize(untaken + fresh);
+        for (size_t i = 0; i < untaken; ++i) out.cont[i] = ck.cont[ncont - untaken + i];
+        if (fresh)
+            NQ_CUDA(cudaMemcpy(out.cont.data() + untaken, c.aux.p, fresh * 16, cudaMemcpyDeviceToHost));
+        rc = write_checkpoint(checkpoint_path, out);
+        if (rc) return rc;
+        if (stats) stats->total_ms = now_ms() - t0;
+        return NQ_OK;
+    }
+    *total = 2 * partial;
+    *done = 1;
+    if (have) std::remove(checkpoint_path);
+    if (stats) stats->total_ms = now_ms() - t0;
+    return NQ_OK;
 }
 
 int nq_count_learned(int N, int rows, nq_mlp *m, const nq_config *cfg, uint64_t *total, nq_stats *stats) {

@@ -46,12 +46,13 @@ enum CtlWord : int {
     kCtlDone = 1,      // CTAs finished
     kCtlError = 2,     // error bits (kErr*)
     kCtlTimeout = 3,   // set when the deadline stopped the kernel
-    kCtlWords = 4,
+    kCtlCont = 4,      // continuation entries written at a deadline stop
+    kCtlWords = 5,
 };
-enum : unsigned long long { kErrDepth = 1ull };
+enum : unsigned long long { kErrDepth = 1ull, kErrContOverflow = 2ull };
 // Bits of *status_out: a task needed more stack levels than the launch had
 // (it was skipped), and/or the run-time limit stopped the kernel early.
-enum : unsigned long long { kStatDepth = 1ull, kStatTimeout = 2ull };
+enum : unsigned long long { kStatDepth = 1ull, kStatTimeout = 2ull, kStatContOverflow = 4ull };
 
 struct DfsParams {
     const uint32_t *cols;      // task column masks (reference `cur`)
@@ -77,6 +78,18 @@ struct DfsParams {
     uint32_t k_one, k_two, k_mone;   // 1, 2, -1 (see dfs_step)
     unsigned long long *cta_times;   // optional [2*gridDim.x]: %globaltimer at CTA start and end
     int layout;                      // stack layout: 0 interleaved (default), 1 lane-major
+    // Resumable runs.  Queue positions [0, n_cont_in) are continuation entries
+    // (a lane's saved level: cols with the off-board bits set, ld, rd, untried
+    // columns); position n_cont_in + j is task list position task_base + j.
+    const uint4 *cont_in;
+    const uint32_t *cont_in_owner;   // optional owners of the continuation entries
+    long long n_cont_in;
+    long long task_base;
+    // At a deadline stop every lane writes its unfinished levels here (if not
+    // null): the current level and each stacked level, in kCtlCont order.
+    uint4 *cont_out;
+    uint32_t *cont_out_owner;        // optional
+    long long cont_cap;
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -260,7 +273,9 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
     uint32_t cnt = 0, it = 0;
     uint32_t owner = kNoOwner;
     unsigned long long tot = 0, tot_nodes = 0;
-    bool queue_live = true;
+    const long long qlen = p.n_cont_in + p.ntasks - p.task_base;
+    bool queue_live = qlen > 0;
+    bool timed_out = false;
     unsigned long long deadline = 0;
     if (p.limit_ns) {
         unsigned long long t0 = 0;
@@ -294,6 +309,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
             now = __shfl_sync(kFull, now, 0);
             if (now > deadline) {
                 if (lane == 0) atomicExch(p.ctl + kCtlTimeout, 1ull);
+                timed_out = true;
                 break;
             }
         }
@@ -308,22 +324,37 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                 unsigned long long b = 0;
                 if ((int)lane == leader) b = atomicAdd(p.ctl + kCtlHead, (unsigned long long)nidle);
                 b = __shfl_sync(kFull, b, leader);
-                if (b + (unsigned long long)nidle >= (unsigned long long)p.ntasks) queue_live = false;
+                if (b + (unsigned long long)nidle >= (unsigned long long)qlen) queue_live = false;
                 if (avail == 0) {
                     const unsigned long long q = b + (unsigned long long)__popc(idle & lanemask_lt());
-                    const long long t = (q < (unsigned long long)p.ntasks)
-                                            ? (p.order ? (long long)__ldg(p.order + q) : (long long)q)
-                                            : -1;
-                    // A permutation entry out of range is skipped, never dereferenced.
-                    if (t >= 0 && t < p.ntasks) {
+                    if (q < (unsigned long long)p.n_cont_in) {
+                        // a level saved by an earlier, interrupted run
                         sp = bot = my_base;
-                        const uint32_t done = load_task(p, t, cols, ld, rd, avail);
-                        const uint32_t own = p.owner_of ? __ldg(p.owner_of + t) : (uint32_t)t;
-                        if (PER_OWNER) {
-                            if (done) atomicAdd(p.out_cnt + own, (unsigned long long)done);
-                            if (avail) owner = own;
+                        const uint4 e = p.cont_in[q];
+                        const int need = __popc(~e.x) - 1;
+                        if (need > p.levels) {
+                            atomicOr(p.ctl + kCtlError, kErrDepth);
+                        } else {
+                            cols = e.x;
+                            ld = e.y;
+                            rd = e.z;
+                            avail = e.w;
+                            if (PER_OWNER && avail) owner = p.cont_in_owner ? p.cont_in_owner[q] : 0u;
                         }
-                        tot += done;
+                    } else if (q < (unsigned long long)qlen) {
+                        const long long pos = p.task_base + (long long)(q - (unsigned long long)p.n_cont_in);
+                        const long long t = p.order ? (long long)__ldg(p.order + pos) : pos;
+                        // A permutation entry out of range is skipped, never dereferenced.
+                        if (t >= 0 && t < p.ntasks) {
+                            sp = bot = my_base;
+                            const uint32_t done = load_task(p, t, cols, ld, rd, avail);
+                            const uint32_t own = p.owner_of ? __ldg(p.owner_of + t) : (uint32_t)t;
+                            if (PER_OWNER) {
+                                if (done) atomicAdd(p.out_cnt + own, (unsigned long long)done);
+                                if (avail) owner = own;
+                            }
+                            tot += done;
+                        }
                     }
                 }
                 // Lanes whose task was empty are still idle: refill again.
@@ -382,6 +413,31 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
 #pragma unroll
                 for (int u = 0; u < UNROLL; ++u) dfs_step<NODES, VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
                 if (__all_sync(kFull, avail == 0)) break;
+            }
+        }
+    }
+
+    // Deadline stop: save every unfinished level so a later run can resume.
+    // The current level keeps its untried columns; every stacked level does
+    // too (only levels with untried columns are ever pushed).
+    if (timed_out && p.cont_out) {
+        const uint32_t nstk = (sp - bot) / stride;
+        const uint32_t mine = (avail != 0 ? 1u : 0u) + nstk;
+        unsigned long long at = 0;
+        if (mine) at = atomicAdd(p.ctl + kCtlCont, (unsigned long long)mine);
+        if (mine && at + mine > (unsigned long long)p.cont_cap) {
+            atomicOr(p.ctl + kCtlError, kErrContOverflow);
+        } else if (mine) {
+            if (avail) {
+                p.cont_out[at] = make_uint4(cols, ld, rd, avail);
+                if (p.cont_out_owner) p.cont_out_owner[at] = owner;
+                ++at;
+            }
+            for (uint32_t a = bot; a != sp; a += stride, ++at) {
+                uint32_t x, y, z, w;
+                lds128(a, x, y, z, w);
+                p.cont_out[at] = make_uint4(x, y, z, w);
+                if (p.cont_out_owner) p.cont_out_owner[at] = owner;
             }
         }
     }
@@ -452,7 +508,8 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
             if (NODES) *p.nodes_out = an;
             const unsigned long long err = *((volatile unsigned long long *)(p.ctl + kCtlError));
             const unsigned long long tmo = *((volatile unsigned long long *)(p.ctl + kCtlTimeout));
-            *p.status_out = ((err & kErrDepth) ? kStatDepth : 0ull) | (tmo ? kStatTimeout : 0ull);
+            *p.status_out = ((err & kErrDepth) ? kStatDepth : 0ull) | (tmo ? kStatTimeout : 0ull) |
+                            ((err & kErrContOverflow) ? kStatContOverflow : 0ull);
         }
     }
 }

@@ -4,7 +4,10 @@
 #include <stdlib.h>
 #include <sys/time.h>
 
+#include <string.h>
+
 #include "n_queens.h"
+#include "n_queens_b200.h"
 #include "timefmt.h"
 
 // Deepest per-lane stack the library accepts for the CLI's range of N (the
@@ -13,8 +16,17 @@ static const int kStackLevels = 30;
 
 int main(int argc, char *argv[]) {
     if (argc < 3) {
-        printf("usage: %s N rows\n", argv[0]);
+        printf("usage: %s N rows [--checkpoint PATH [--slice-ms MS]]\n", argv[0]);
         return -1;
+    }
+    // Optional resumable mode (not in the reference): the count runs in
+    // slices of MS milliseconds and saves its state to PATH after each one, so
+    // an interrupted run continues where it stopped when started again.
+    const char *ckpt = nullptr;
+    unsigned slice_ms = 600000;
+    for (int a = 3; a + 1 < argc; a += 2) {
+        if (!strcmp(argv[a], "--checkpoint")) ckpt = argv[a + 1];
+        else if (!strcmp(argv[a], "--slice-ms")) slice_ms = (unsigned)strtoul(argv[a + 1], nullptr, 10);
     }
     int N = atoi(argv[1]);
     if (N < 2 || N > 28) {
@@ -42,7 +54,29 @@ int main(int argc, char *argv[]) {
     struct timeval start, end;
     nqb::print_with_time("===============================================================\n");
     gettimeofday(&start, NULL);
-    long long sum = cuda_n_queens(N, rows);
+    long long sum = 0;
+    if (ckpt) {
+        nq_config cfg;
+        memset(&cfg, 0, sizeof(cfg));
+        cfg.time_limit_ms = slice_ms;
+        for (int slice = 1;; ++slice) {
+            uint64_t total = 0;
+            int done = 0;
+            const int rc = nq_count_resumable(N, rows, &cfg, ckpt, &total, &done, nullptr);
+            if (rc != NQ_OK) {
+                printf("n_queens_b200: %s (%s)\n", nq_status_string(rc), nq_last_error());
+                sum = -1;
+                break;
+            }
+            if (done) {
+                sum = (long long)total;
+                break;
+            }
+            nqb::print_with_time("slice %d saved to %s\n", slice, ckpt);
+        }
+    } else {
+        sum = cuda_n_queens(N, rows);
+    }
     gettimeofday(&end, NULL);
     nqb::print_with_time("cuda %d queens result %lld, calc time: [%.2fms]\n", N, sum, nqb::time_diff_ms(start, end));
     nqb::print_with_time("===============================================================\n");

@@ -132,3 +132,24 @@ def test_cli_without_gpu():
     assert "Failed to find any gpu!" in out
     assert re.search(r"^\[\d{4}-\d\d-\d\d \d\d:\d\d:\d\d\.\d{3}\] cuda 12 queens result -1, calc time: \[",
                      out, re.M)
+
+
+def test_resumable_rejects_foreign_or_broken_checkpoints(tmp_path):
+    # Checked before any device work, so this runs without a GPU.
+    import struct
+    p = tmp_path / "ck"
+    hdr = b"NQB200CK" + struct.pack("<IiiiqqQQq", 1, 10, 3, 0, 100, 5, 7, 1, 0)
+    p.write_bytes(hdr)
+    t = ctypes.c_uint64(0)
+    d = ctypes.c_int(0)
+    rc = nq.lib.nq_count_resumable(11, 3, None, str(p).encode(), ctypes.byref(t), ctypes.byref(d), None)
+    assert rc == nq.NQ_ERR_ARG and "N=10" in nq.last_error()
+    p.write_bytes(hdr[:-3])                                   # truncated
+    assert nq.lib.nq_count_resumable(10, 3, None, str(p).encode(), ctypes.byref(t), ctypes.byref(d), None) \
+        == nq.NQ_ERR_ARG
+    p.write_bytes(b"XXXXXXXX" + hdr[8:])                      # wrong magic
+    assert nq.lib.nq_count_resumable(10, 3, None, str(p).encode(), ctypes.byref(t), ctypes.byref(d), None) \
+        == nq.NQ_ERR_ARG
+    p.write_bytes(hdr + b"z")                                 # trailing bytes
+    assert nq.lib.nq_count_resumable(10, 3, None, str(p).encode(), ctypes.byref(t), ctypes.byref(d), None) \
+        == nq.NQ_ERR_ARG
