@@ -168,6 +168,8 @@ int ensure_ready(Ctx &c, int dev) {
             for (int v = 0; v < 3; ++v)
                 NQ_CUDA(cudaFuncSetAttribute(pick_kernel(po, nd, v), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              c.smem_optin - static_smem));
+    NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, 1, 8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 c.smem_optin - static_smem));
     c.ready = true;
     return NQ_OK;
 }
@@ -838,6 +840,14 @@ int nq_count_resumable(int N, int rows, const nq_config *cfg, const char *checkp
     Launch L;
     rc = plan_launch(c, cfg, N - 1 - rows, false, false, L);
     if (rc) return rc;
+    {
+        // the resumable instantiation may fit fewer CTAs per SM
+        int per_sm = 0;
+        NQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dfs_kernel<false, false, 1, 8, true>,
+                                                              L.threads, L.smem));
+        if (per_sm <= 0) return NQ_ERR_ARG;
+        L.grid = std::min(L.grid, c.sms * std::min(per_sm, kMaxBlocksPerSm));
+    }
     fill_stats_launch(stats, L);
     // room for every lane's unfinished levels: the current one + one per slot
     const size_t cap = (size_t)L.grid * L.threads * (L.levels + 1);
@@ -852,9 +862,14 @@ int nq_count_resumable(int N, int rows, const nq_config *cfg, const char *checkp
     p.task_base = have ? ck.cursor : 0;
     p.cont_out = (uint4 *)c.aux.p;
     p.cont_cap = (long long)cap;
+    p.levels = L.levels;
+    p.inner = L.inner;
+    p.steal = L.steal;
+    p.layout = L.layout;
     NQ_CUDA(cudaEventRecord(c.ev[1], c.stream));
-    rc = enqueue_dfs(c, p, L, false, false, c.stream);
-    if (rc) return rc;
+    NQ_CUDA(cudaMemsetAsync(p.ctl, 0, kCtlWords * sizeof(unsigned long long), c.stream));
+    dfs_kernel<false, false, 1, 8, true><<<L.grid, L.threads, L.smem, c.stream>>>(p);
+    NQ_CUDA(cudaGetLastError());
     NQ_CUDA(cudaEventRecord(c.ev[2], c.stream));
     unsigned long long words[kWordBlocks];
     NQ_CUDA(cudaMemcpyAsync(words, c.d_ctl, sizeof(words), cudaMemcpyDeviceToHost, c.stream));

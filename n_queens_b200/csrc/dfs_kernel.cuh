@@ -248,7 +248,10 @@ __device__ __forceinline__ uint32_t load_task(const DfsParams &p, long long t, u
     return 0;
 }
 
-template <bool PER_OWNER, bool NODES, int VAR, int UNROLL>
+// RESUME adds the continuation queue and the deadline dump; it is a separate
+// instantiation so that the plain count kernel carries none of that code
+// (it measurably changed the code generated for the DFS loop).
+template <bool PER_OWNER, bool NODES, int VAR, int UNROLL, bool RESUME = false>
 __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long red_cnt[32];
@@ -273,7 +276,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
     uint32_t cnt = 0, it = 0;
     uint32_t owner = kNoOwner;
     unsigned long long tot = 0, tot_nodes = 0;
-    const long long qlen = p.n_cont_in + p.ntasks - p.task_base;
+    const long long qlen = RESUME ? p.n_cont_in + p.ntasks - p.task_base : p.ntasks;
     bool queue_live = qlen > 0;
     bool timed_out = false;
     unsigned long long deadline = 0;
@@ -309,7 +312,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
             now = __shfl_sync(kFull, now, 0);
             if (now > deadline) {
                 if (lane == 0) atomicExch(p.ctl + kCtlTimeout, 1ull);
-                timed_out = true;
+                if (RESUME) timed_out = true;
                 break;
             }
         }
@@ -327,7 +330,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                 if (b + (unsigned long long)nidle >= (unsigned long long)qlen) queue_live = false;
                 if (avail == 0) {
                     const unsigned long long q = b + (unsigned long long)__popc(idle & lanemask_lt());
-                    if (q < (unsigned long long)p.n_cont_in) {
+                    if (RESUME && q < (unsigned long long)p.n_cont_in) {
                         // a level saved by an earlier, interrupted run
                         sp = bot = my_base;
                         const uint4 e = p.cont_in[q];
@@ -342,7 +345,8 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                             if (PER_OWNER && avail) owner = p.cont_in_owner ? p.cont_in_owner[q] : 0u;
                         }
                     } else if (q < (unsigned long long)qlen) {
-                        const long long pos = p.task_base + (long long)(q - (unsigned long long)p.n_cont_in);
+                        const long long pos =
+                            RESUME ? p.task_base + (long long)(q - (unsigned long long)p.n_cont_in) : (long long)q;
                         const long long t = p.order ? (long long)__ldg(p.order + pos) : pos;
                         // A permutation entry out of range is skipped, never dereferenced.
                         if (t >= 0 && t < p.ntasks) {
@@ -420,7 +424,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
     // Deadline stop: save every unfinished level so a later run can resume.
     // The current level keeps its untried columns; every stacked level does
     // too (only levels with untried columns are ever pushed).
-    if (timed_out && p.cont_out) {
+    if (RESUME && timed_out && p.cont_out) {
         const uint32_t nstk = (sp - bot) / stride;
         const uint32_t mine = (avail != 0 ? 1u : 0u) + nstk;
         unsigned long long at = 0;
