@@ -2,6 +2,7 @@
 expander order, on one GPU (the comparison the cost model exists for).
 
     python -m n_queens_b200.compare_schedules --N 22 --k 6 [--repeats 1] [--json out.json]
+                                              [--schedules plain,learned]
 
 Builds the cost model once (solver-logged node counts at N=16..18, fine-tuned
 on a seeded 5% sample of the target's prefixes), then alternates plain and
@@ -26,13 +27,19 @@ def main():
     ap.add_argument("--repeats", type=int, default=1)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--json", default=None)
+    ap.add_argument("--schedules", default="plain,learned", help="comma list of plain, learned")
     args = ap.parse_args()
-    t = time.perf_counter()
-    model, rep = learned.build_cost_model(args.N, k=args.k, seed=args.seed)
-    out = {"N": args.N, "k": args.k, "model_build_s": time.perf_counter() - t, "build": rep.__dict__, "runs": []}
-    print(json.dumps({"model_build_s": out["model_build_s"], "holdout_spearman": rep.holdout_spearman}), flush=True)
+    names = [x for x in args.schedules.split(",") if x]
+    out = {"N": args.N, "k": args.k, "runs": []}
+    model = None
+    if "learned" in names:
+        t = time.perf_counter()
+        model, rep = learned.build_cost_model(args.N, k=args.k, seed=args.seed)
+        out.update(model_build_s=time.perf_counter() - t, build=rep.__dict__)
+        print(json.dumps({"model_build_s": out["model_build_s"], "holdout_spearman": rep.holdout_spearman}),
+              flush=True)
     for it in range(args.repeats):
-        for name in ("plain", "learned"):
+        for name in names:
             t = time.perf_counter()
             if name == "plain":
                 r = count(args.N, args.k, config=dict(timing=1))
@@ -48,7 +55,8 @@ def main():
     if args.json:
         with open(args.json, "w") as f:
             json.dump(out, f, indent=1)
-    model.close()
+    if model is not None:
+        model.close()
 
 
 if __name__ == "__main__":
