@@ -76,7 +76,9 @@ typedef struct nq_config {
     int timing;             /* non-zero: host entries record per-CTA start/end times and fill the
                                makespan / tail fields of nq_stats */
     int layout;             /* NQ_LAYOUT_INTERLEAVED (default) or NQ_LAYOUT_LANE_MAJOR */
-    int reserved[4];
+    int device_expand;      /* nq_count: non-zero builds the prefix tasks on the device (nq_expand_device)
+                               instead of on the host + H2D copy */
+    int reserved[3];
 } nq_config;
 
 /* Timings and sizes of one call (all optional outputs). */
@@ -128,6 +130,15 @@ int nq_device_count(int *count);
  * threads <= 0 uses every host core. */
 int nq_expand(int N, int rows, uint32_t *cols, uint32_t *ld, uint32_t *rd, int64_t cap, int64_t *n_tasks,
               int threads);
+
+/* The same expansion on the device (no counterpart in the reference): the
+ * host enumerates the reference-ordered placements of the first min(rows, 4)
+ * rows, then a count pass, a scan and a write pass on `device` produce the
+ * prefixes into the caller's device arrays, in the same order as nq_expand.
+ * Writes at most cap tasks, *n_tasks receives the full count; synchronises
+ * `stream` (NULL = legacy default) once, to learn that count. */
+int nq_expand_device(int N, int rows, uint32_t *d_cols, uint32_t *d_ld, uint32_t *d_rd, int64_t cap,
+                     int64_t *n_tasks, int device, void *stream);
 
 /* Whole-board count.  Replaces cuda_n_queens (src/n_queens_cuda.cu:84-186)
  * on one device: expand, upload, count, and return 2 x the sum of the

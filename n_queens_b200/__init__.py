@@ -67,7 +67,8 @@ class Config(ctypes.Structure):
         ("device", ctypes.c_int),
         ("timing", ctypes.c_int),
         ("layout", ctypes.c_int),
-        ("reserved", ctypes.c_int * 4),
+        ("device_expand", ctypes.c_int),
+        ("reserved", ctypes.c_int * 3),
     ]
 
 
@@ -134,6 +135,9 @@ def _load() -> ctypes.CDLL:
     L.nq_device_count.argtypes = [ctypes.POINTER(ctypes.c_int)]
     L.nq_expand.restype = ctypes.c_int
     L.nq_expand.argtypes = [ctypes.c_int, ctypes.c_int, _u32p, _u32p, _u32p, ctypes.c_int64, _i64p, ctypes.c_int]
+    L.nq_expand_device.restype = ctypes.c_int
+    L.nq_expand_device.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                   ctypes.c_int64, _i64p, ctypes.c_int, ctypes.c_void_p]
     L.nq_count.restype = ctypes.c_int
     L.nq_count.argtypes = [ctypes.c_int, ctypes.c_int, _cfgp, _u64p, _u64p, _stp]
     L.nq_count_resumable.restype = ctypes.c_int
@@ -168,7 +172,8 @@ def _load() -> ctypes.CDLL:
 lib = _load()
 
 # Every symbol the C header declares (checked by the CPU test suite).
-EXPORTS = ("nq_abi_version", "nq_status_string", "nq_last_error", "nq_device_count", "nq_expand", "nq_count",
+EXPORTS = ("nq_abi_version", "nq_status_string", "nq_last_error", "nq_device_count", "nq_expand",
+           "nq_expand_device", "nq_count",
            "nq_count_resumable",
            "nq_count_tasks", "nq_count_tasks_device", "nq_count_tasks_device_noalloc", "nq_count_batch",
            "nq_batch_create", "nq_batch_run", "nq_batch_destroy", "nq_batch_autotune",

@@ -136,6 +136,7 @@ struct Ctx {
     DevBuf tasks;                         // cols | ld | rd (uint32 SoA)
     DevBuf aux;                           // order, owners, task_n, per-task outputs
     HostBuf h_tasks;                      // pinned staging for the expander
+    DevBuf expand_scratch;                // seeds, counts, offsets of the device expander
 };
 
 Ctx g_ctx[kMaxDevices];
@@ -731,6 +732,35 @@ int nq_expand(int N, int rows, uint32_t *cols, uint32_t *ld, uint32_t *rd, int64
     return NQ_OK;
 }
 
+int nq_expand_device(int N, int rows, uint32_t *d_cols, uint32_t *d_ld, uint32_t *d_rd, int64_t cap,
+                     int64_t *n_tasks, int device, void *stream) {
+    if (N < 2 || N > NQ_MAX_N || rows < 1 || rows > N || !n_tasks || cap < 0) return NQ_ERR_ARG;
+    if (cap > 0 && (!d_cols || !d_ld || !d_rd)) return NQ_ERR_ARG;
+    Ctx *cp = nullptr;
+    int rc = lock_device(device, cp);
+    if (rc) return rc;
+    Ctx &c = *cp;
+    std::lock_guard<std::mutex> lock(c.mu);
+    rc = ensure_ready(c, device);
+    if (rc) return rc;
+    NQ_CUDA(expand_prefixes_device(N, rows, d_cols, d_ld, d_rd, cap, n_tasks, &c.expand_scratch.p,
+                                   &c.expand_scratch.cap, (cudaStream_t)stream));
+    return NQ_OK;
+}
+
+// Expands (N, rows) into the context's task buffer on the device.
+int device_expand_into_ctx(Ctx &c, int N, int rows, int64_t &n) {
+    NQ_CUDA(expand_prefixes_device(N, rows, nullptr, nullptr, nullptr, 0, &n, &c.expand_scratch.p,
+                                   &c.expand_scratch.cap, c.stream));
+    int rc = c.tasks.grow((size_t)std::max<int64_t>(n, 1) * 16 + 256);
+    if (rc) return rc;
+    uint32_t *d = (uint32_t *)c.tasks.p;
+    int64_t n2 = 0;
+    NQ_CUDA(expand_prefixes_device(N, rows, d, d + n, d + 2 * n, n, &n2, &c.expand_scratch.p, &c.expand_scratch.cap,
+                                   c.stream));
+    return n2 == n ? NQ_OK : NQ_ERR_CUDA;
+}
+
 int nq_count(int N, int rows, const nq_config *cfg, uint64_t *total, uint64_t *nodes, nq_stats *stats) {
     const double t0 = now_ms();
     if (stats) memset(stats, 0, sizeof(*stats));
@@ -756,32 +786,43 @@ int nq_count(int N, int rows, const nq_config *cfg, uint64_t *total, uint64_t *n
     if (rc) return rc;
 
     const double te = now_ms();
-    uint32_t *h = nullptr;
-    int grow_rc = NQ_OK;
-    const int64_t n = expand_prefixes_to(
-        N, rows,
-        [&](int64_t total_tasks, uint32_t **pc, uint32_t **pl, uint32_t **pr, int64_t *cap) {
-            grow_rc = c.h_tasks.grow((size_t)std::max<int64_t>(total_tasks, 1) * 12);
-            if (grow_rc) return false;
-            h = (uint32_t *)c.h_tasks.p;
-            *pc = h;
-            *pl = h + total_tasks;
-            *pr = h + 2 * total_tasks;
-            *cap = total_tasks;
-            return true;
-        },
-        0);
-    if (grow_rc) return grow_rc;
-    if (n < 0) return NQ_ERR_ARG;
-    if (stats) {
-        stats->expand_ms = now_ms() - te;
-        stats->tasks = n;
+    int64_t n = 0;
+    if (cfg && cfg->device_expand) {
+        rc = device_expand_into_ctx(c, N, rows, n);
+        if (rc) return rc;
+        if (stats) {
+            stats->expand_ms = now_ms() - te;
+            stats->tasks = n;
+        }
+        NQ_CUDA(cudaEventRecord(c.ev[0], c.stream));
+    } else {
+        uint32_t *h = nullptr;
+        int grow_rc = NQ_OK;
+        n = expand_prefixes_to(
+            N, rows,
+            [&](int64_t total_tasks, uint32_t **pc, uint32_t **pl, uint32_t **pr, int64_t *cap) {
+                grow_rc = c.h_tasks.grow((size_t)std::max<int64_t>(total_tasks, 1) * 12);
+                if (grow_rc) return false;
+                h = (uint32_t *)c.h_tasks.p;
+                *pc = h;
+                *pl = h + total_tasks;
+                *pr = h + 2 * total_tasks;
+                *cap = total_tasks;
+                return true;
+            },
+            0);
+        if (grow_rc) return grow_rc;
+        if (n < 0) return NQ_ERR_ARG;
+        if (stats) {
+            stats->expand_ms = now_ms() - te;
+            stats->tasks = n;
+        }
+        rc = c.tasks.grow((size_t)std::max<int64_t>(n, 1) * 12);
+        if (rc) return rc;
+        NQ_CUDA(cudaEventRecord(c.ev[0], c.stream));
+        if (n) NQ_CUDA(cudaMemcpyAsync(c.tasks.p, h, (size_t)n * 12, cudaMemcpyHostToDevice, c.stream));
     }
-    rc = c.tasks.grow((size_t)std::max<int64_t>(n, 1) * 12);
-    if (rc) return rc;
     uint32_t *d = (uint32_t *)c.tasks.p;
-    NQ_CUDA(cudaEventRecord(c.ev[0], c.stream));
-    if (n) NQ_CUDA(cudaMemcpyAsync(d, h, (size_t)n * 12, cudaMemcpyHostToDevice, c.stream));
     uint64_t sum = 0, nd = 0;
     rc = count_resident(c, N, d, d + n, d + 2 * n, n, N - 1 - rows, cfg, false, nodes != nullptr, nullptr, nullptr,
                         &sum, &nd, stats, true);

@@ -1,6 +1,7 @@
 // expand.h -- host prefix expansion (see expand.cpp).
 #pragma once
 
+#include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <functional>
@@ -21,5 +22,11 @@ int64_t expand_prefixes_to(int N, int rows, const PrefixSink &sink, int threads)
 // subtasks; returns how many were appended.
 int64_t expand_board(int N, uint32_t c0, uint32_t l0, uint32_t r0, int rows, std::vector<uint32_t> &cols,
                      std::vector<uint32_t> &ld, std::vector<uint32_t> &rd);
+
+// Device expansion into caller device arrays (expand_dev.cu); `scratch` is a
+// device buffer the function grows as needed.  Same output and order as
+// expand_prefixes.
+cudaError_t expand_prefixes_device(int N, int rows, uint32_t *d_cols, uint32_t *d_ld, uint32_t *d_rd, int64_t cap,
+                                   int64_t *n_tasks, void **scratch, size_t *scratch_cap, cudaStream_t stream);
 
 }  // namespace nqb

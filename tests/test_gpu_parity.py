@@ -212,3 +212,31 @@ def test_batch_autotune_sweep(gpu):
     assert best["ms"] == min(e["ms"] for e in table)
     cfg = dict(block_threads=best["block_threads"], layout=best["layout"])
     assert gpu.count_batch(inst, split_rows=best["split_rows"], config=cfg).tolist() == want
+
+
+def test_device_expander_matches_reference_bytes(gpu, golden):
+    import ctypes
+    import hashlib
+    import torch
+    dev = torch.device("cuda:0")
+    for case in golden("expander.json"):
+        N, k = case["N"], case["k"]
+        n = ctypes.c_int64(0)
+        assert gpu.lib.nq_expand_device(N, k, None, None, None, 0, ctypes.byref(n), 0, None) == 0
+        assert n.value == case["tasks"], case
+        bufs = [torch.empty(max(n.value, 1), dtype=torch.int32, device=dev) for _ in range(3)]
+        assert gpu.lib.nq_expand_device(N, k, *(b.data_ptr() for b in bufs), n.value, ctypes.byref(n), 0,
+                                        None) == 0
+        torch.cuda.synchronize()
+        aos = np.stack([b[:n.value].cpu().numpy() for b in bufs], axis=1)
+        assert hashlib.sha256(np.ascontiguousarray(aos).tobytes()).hexdigest() == case["sha256_aos_int32"], case
+
+
+def test_count_with_device_expansion(gpu, golden):
+    pub = golden("published.json")
+    for N, k in [(13, 5), (16, 6), (19, 6)]:
+        r = gpu.count(N, k, config=dict(device_expand=1))
+        assert r.total == pub[str(N)]["total"] and r.stats["tasks"] > 0
+    for N in range(4, 12):
+        for k in range(1, N - 1):
+            assert gpu.count(N, k, config=dict(device_expand=1)).total == oracle.total(N, k), (N, k)
