@@ -204,6 +204,10 @@ def dist_init(n_gpus: int):
     if world > 1:
         import torch.distributed as dist
 
+        if n_gpus > 0:
+            import torch
+
+            torch.cuda.set_device(local)  # each rank's NCCL communicator on its own GPU
         dist.init_process_group("nccl" if n_gpus > 0 else "gloo", timeout=datetime.timedelta(seconds=900))
     return world, rank, local
 

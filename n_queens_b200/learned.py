@@ -1,6 +1,6 @@
 """Learned subtree-cost scheduling (host side).
 
-The pipeline ``north_star`` asks for, on top of the C ABI in mlp.cu/capi.cu:
+The learned scheduling pipeline, on top of the C ABI in mlp.cu/capi.cu:
 
 1. the solver logs per-prefix DFS node counts at small N (``solver_labels``:
    nq_count_tasks with per-task nodes), target = log2(1 + nodes);
