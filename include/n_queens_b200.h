@@ -266,6 +266,12 @@ int nq_mlp_set_params(nq_mlp *m, const float *in);
 /* Predicted log2(1 + nodes) of n tasks of board size N (host arrays). */
 int nq_mlp_predict(nq_mlp *m, int N, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd, int64_t n,
                    float *out);
+/* The same forward on the tensor cores (tcgen05.mma, BF16 operands, FP32
+ * accumulators in TMEM), as nq_schedule_device runs it: the layer-1 outputs
+ * are rounded to BF16 before layer 2, so results differ from nq_mlp_predict
+ * by that rounding. */
+int nq_mlp_predict_tensor(nq_mlp *m, int N, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd, int64_t n,
+                          float *out);
 /* Gradient of the mean squared error over n tasks (per-task board sizes in
  * task_n, targets in log2(1 + nodes)) with respect to the BF16 compute
  * weights, in the flat layout, and the loss.  Changes nothing. */

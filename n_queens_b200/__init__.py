@@ -178,7 +178,7 @@ EXPORTS = ("nq_abi_version", "nq_status_string", "nq_last_error", "nq_device_cou
            "nq_count_tasks", "nq_count_tasks_device", "nq_count_tasks_device_noalloc", "nq_count_batch",
            "nq_batch_create", "nq_batch_run", "nq_batch_destroy", "nq_batch_autotune",
            "nq_mlp_num_params", "nq_mlp_create", "nq_mlp_destroy", "nq_mlp_get_params", "nq_mlp_set_params",
-           "nq_mlp_predict", "nq_mlp_grad", "nq_mlp_train", "nq_schedule_device", "nq_count_learned")
+           "nq_mlp_predict", "nq_mlp_predict_tensor", "nq_mlp_grad", "nq_mlp_train", "nq_schedule_device", "nq_count_learned")
 
 
 def status_string(status: int) -> str:

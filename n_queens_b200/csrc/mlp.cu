@@ -166,6 +166,222 @@ __global__ void __launch_bounds__(128) mlp_predict_kernel(TaskView tv, long long
     }
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core inference (tcgen05).  Per tile of 128 tasks, one CTA of 128
+// threads (thread t = task row t = TMEM lane t):
+//   X (128 x 96 binary, BF16) --tcgen05.mma--> D1 (TMEM, FP32) --relu+b1,
+//   BF16--> H1 (128 x 128, smem) --tcgen05.mma--> D2 (TMEM) --relu+b2, dot W3,
+//   +b3--> out.
+// Operands use the SM100 K-major canonical layout without swizzle: 8-row x
+// 16-byte core matrices, LBO = 128 B between the two core matrices of one
+// K=16 step, SBO = K/8 * 128 B between 8-row groups.  One thread issues the
+// MMAs; completion is signalled through an mbarrier (tcgen05.commit) and every
+// wait on it is bounded (on expiry the kernel sets *err and stops).
+namespace tc {
+
+constexpr uint32_t kSbo1 = (kIn / 8) * 128;   // 1536 B
+constexpr uint32_t kSbo2 = (kH1 / 8) * 128;   // 2048 B
+constexpr uint32_t kOffB1 = 0;                 // W1: 128 units x 96  (24 KiB)
+constexpr uint32_t kOffB2 = kOffB1 + kH1 * kSbo1 / 8;  // 24576: W2: 128 x 128 (32 KiB)
+constexpr uint32_t kOffA = kOffB2 + kH2 * kSbo2 / 8;   // 57344: X / H1 tile (32 KiB)
+constexpr uint32_t kOffBias = kOffA + 128 * kSbo2 / 8;  // 90112: b1, b2, w3 (fp32)
+constexpr uint32_t kOffBar = kOffBias + 3 * 128 * 4;    // 91648: mbarrier (8 B)
+constexpr uint32_t kOffTmem = kOffBar + 8;              // TMEM base address word
+constexpr uint32_t kSmemBytes = kOffTmem + 8;
+constexpr uint32_t kTmemCols = 256;  // D1 at column 0, D2 at column 128
+// Instruction descriptor, kind::f16: D F32, A and B BF16, both K-major,
+// N = 128 (N>>3 at bit 17), M = 128 (M>>4 at bit 24).
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr unsigned long long kWaitLimit = 1ull << 22;  // a few seconds at most
+
+__host__ __device__ constexpr uint32_t off_kmajor(uint32_t row, uint32_t k, uint32_t sbo) {
+    return (row >> 3) * sbo + (k >> 3) * 128u + (row & 7u) * 16u + (k & 7u) * 2u;
+}
+static_assert(off_kmajor(127, 95, kSbo1) < kOffB2 - kOffB1, "W1 tile bounds");
+static_assert(off_kmajor(127, 127, kSbo2) < kOffA - kOffB2, "W2 tile bounds");
+static_assert(off_kmajor(127, 127, kSbo2) < kOffBias - kOffA, "A tile bounds");
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);  // version 1; base offset 0; no swizzle
+}
+
+__device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t da, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// Bounded wait for the mbarrier phase with the given parity; false on expiry.
+__device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t parity) {
+    for (unsigned long long i = 0; i < kWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);  // a -> low half
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+__device__ __forceinline__ void sts128(uint32_t addr, uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
+    asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(x), "r"(y), "r"(z), "r"(w) : "memory");
+}
+
+}  // namespace tc
+
+__global__ void __launch_bounds__(128, 1)
+    mlp_predict_tc_kernel(TaskView tv, long long n, const Weights *w, float *out, int *err) {
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(tc_smem);
+    const uint32_t t = threadIdx.x, warp = t >> 5;
+    float *bias = reinterpret_cast<float *>(tc_smem + tc::kOffBias);
+    const uint32_t bar = base + tc::kOffBar;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tc_smem + tc::kOffTmem);
+
+    // Weights into the canonical operand layouts (BF16 copies as stored).
+    for (uint32_t i = t; i < (uint32_t)(kH1 * kIn); i += blockDim.x) {
+        const uint32_t unit = i / kIn, k = i % kIn;
+        *reinterpret_cast<__nv_bfloat16 *>(tc_smem + tc::kOffB1 + tc::off_kmajor(unit, k, tc::kSbo1)) =
+            w->w1t[k * kH1 + unit];
+    }
+    for (uint32_t i = t; i < (uint32_t)(kH2 * kH1); i += blockDim.x) {
+        const uint32_t unit = i / kH1, k = i % kH1;
+        *reinterpret_cast<__nv_bfloat16 *>(tc_smem + tc::kOffB2 + tc::off_kmajor(unit, k, tc::kSbo2)) =
+            w->w2[unit * kH1 + k];
+    }
+    bias[t] = w->b1[t];
+    bias[128 + t] = w->b2[t];
+    bias[256 + t] = __bfloat162float(w->w3[t]);
+    const float b3 = w->b3;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(base + tc::kOffTmem),
+                     "r"(tc::kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t lane_off = (warp * 32u) << 16;  // this warp's TMEM lanes
+    const uint32_t d1 = tmem, d2 = tmem + 128;
+    uint32_t phase = 0;
+    __shared__ int s_fail;
+    if (t == 0) s_fail = 0;
+    __syncthreads();
+
+    for (long long g0 = (long long)blockIdx.x * 128; g0 < n; g0 += (long long)gridDim.x * 128) {
+        // ---- X row of this thread's task (zeros past the end)
+        uint32_t m0 = 0, m1 = 0, m2 = 0;
+        if (g0 + t < n) load_masks(tv, g0 + t, m0, m1, m2);
+        const uint32_t masks[3] = {m0, m1, m2};
+#pragma unroll
+        for (int c = 0; c < kIn / 8; ++c) {
+            const uint32_t byte = (masks[c >> 2] >> ((c & 3) * 8)) & 0xFFu;
+            uint32_t q[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                q[j] = ((byte >> (2 * j)) & 1u ? 0x3F80u : 0u) | ((byte >> (2 * j + 1)) & 1u ? 0x3F800000u : 0u);
+            tc::sts128(base + tc::kOffA + tc::off_kmajor(t, 8 * c, tc::kSbo1), q[0], q[1], q[2], q[3]);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        // ---- layer 1 on the tensor cores: D1 = X * W1^T, K = 96 in 6 steps
+        if (t == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int kk = 0; kk < kIn / 16; ++kk)
+                tc::mma(d1, tc::smem_desc(base + tc::kOffA + kk * 256, 128, tc::kSbo1),
+                        tc::smem_desc(base + tc::kOffB1 + kk * 256, 128, tc::kSbo1), kk > 0);
+            tc::commit(bar);
+        }
+        if (!tc::wait_phase(bar, phase)) s_fail = 1;
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (s_fail) break;
+        // ---- relu(D1 + b1) -> BF16 -> H1 rows (the A operand of layer 2)
+#pragma unroll 1
+        for (int c = 0; c < kH1 / 16; ++c) {
+            float v[16];
+            tc::ld16(d1 + lane_off + 16 * c, v);
+            uint32_t q[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                q[j] = tc::pack_bf16(fmaxf(v[2 * j] + bias[16 * c + 2 * j], 0.f),
+                                     fmaxf(v[2 * j + 1] + bias[16 * c + 2 * j + 1], 0.f));
+            tc::sts128(base + tc::kOffA + tc::off_kmajor(t, 16 * c, tc::kSbo2), q[0], q[1], q[2], q[3]);
+            tc::sts128(base + tc::kOffA + tc::off_kmajor(t, 16 * c + 8, tc::kSbo2), q[4], q[5], q[6], q[7]);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        // ---- layer 2: D2 = H1 * W2^T, K = 128 in 8 steps
+        if (t == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int kk = 0; kk < kH1 / 16; ++kk)
+                tc::mma(d2, tc::smem_desc(base + tc::kOffA + kk * 256, 128, tc::kSbo2),
+                        tc::smem_desc(base + tc::kOffB2 + kk * 256, 128, tc::kSbo2), kk > 0);
+            tc::commit(bar);
+        }
+        if (!tc::wait_phase(bar, phase)) s_fail = 1;
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (s_fail) break;
+        // ---- layer 3: sum_j relu(D2 + b2)_j * w3_j + b3
+        float acc = 0.f;
+#pragma unroll 1
+        for (int c = 0; c < kH2 / 16; ++c) {
+            float v[16];
+            tc::ld16(d2 + lane_off + 16 * c, v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                acc = fmaf(fmaxf(v[j] + bias[128 + 16 * c + j], 0.f), bias[256 + 16 * c + j], acc);
+        }
+        if (g0 + t < n) out[g0 + t] = acc + b3;
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+    }
+    if (s_fail && t == 0) atomicExch(err, 1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tc::kTmemCols));
+}
+
 // Shared memory of the training kernel (about 216 KiB; one CTA per SM).
 struct TrainSmem {
     __nv_bfloat16 w1t[kIn * kH1];    // 24 KiB
@@ -397,6 +613,7 @@ struct nq_mlp {
     float *grad_part = nullptr;
     int grad_parts_cap = 0;
     float *gsum = nullptr;  // summed gradient (nq_mlp_grad)
+    int *tc_err = nullptr;  // set by the tensor-core kernel when an MMA wait expires
     float *loss_part = nullptr;
     void *data = nullptr;
     size_t data_cap = 0;
@@ -494,6 +711,15 @@ int launch_train(nq_mlp *m, const TaskView &tv, const float *target, long long b
     return NQ_OK;
 }
 
+// Tensor-core forward over n device-resident tasks of board size N.
+int launch_predict_tc(nq_mlp *m, const TaskView &tv, long long n, float *d_out, cudaStream_t s) {
+    const long long tiles = (n + 127) / 128;
+    const int grid = (int)std::min<long long>(tiles, (long long)m->sms * 2);
+    mlp_predict_tc_kernel<<<grid, 128, tc::kSmemBytes, s>>>(tv, n, m->w, d_out, m->tc_err);
+    MLP_CUDA(cudaGetLastError());
+    return NQ_OK;
+}
+
 int check_model(nq_mlp *m) {
     if (!m) return NQ_ERR_ARG;
     MLP_CUDA(cudaSetDevice(m->device));
@@ -526,6 +752,10 @@ int nq_mlp_create(int device, uint64_t seed, nq_mlp **out) {
     if (e == cudaSuccess) e = cudaMalloc(&m->adam2, kParams * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&m->w, sizeof(Weights));
     if (e == cudaSuccess) e = cudaMalloc(&m->gsum, kParams * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&m->tc_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(m->tc_err, 0, sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(mlp_predict_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sizeof(TrainSmem));
     if (e != cudaSuccess) {
@@ -559,6 +789,7 @@ int nq_mlp_destroy(nq_mlp *m) {
     cudaFree(m->adam2);
     cudaFree(m->w);
     cudaFree(m->gsum);
+    cudaFree(m->tc_err);
     cudaFree(m->grad_part);
     cudaFree(m->loss_part);
     cudaFree(m->data);
@@ -610,6 +841,31 @@ int nq_mlp_predict(nq_mlp *m, int N, const uint32_t *cols, const uint32_t *ld, c
     MLP_CUDA(cudaGetLastError());
     MLP_CUDA(cudaMemcpyAsync(out, d_out, (size_t)n * 4, cudaMemcpyDeviceToHost, m->stream));
     MLP_CUDA(cudaStreamSynchronize(m->stream));
+    return NQ_OK;
+}
+
+int nq_mlp_predict_tensor(nq_mlp *m, int N, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd, int64_t n,
+                          float *out) {
+    int rc = check_model(m);
+    if (rc) return rc;
+    if (N < 1 || N > NQ_MAX_N || n < 0 || (n > 0 && (!cols || !ld || !rd || !out))) return NQ_ERR_ARG;
+    if (n == 0) return NQ_OK;
+    std::lock_guard<std::mutex> lock(m->mu);
+    Staged st;
+    rc = stage(m, nullptr, cols, ld, rd, nullptr, n, st);
+    if (rc) return rc;
+    TaskView tv{st.cols, st.ld, st.rd, nullptr, nullptr, N};
+    MLP_CUDA(cudaMemsetAsync(m->tc_err, 0, sizeof(int), m->stream));
+    rc = launch_predict_tc(m, tv, n, st.target, m->stream);
+    if (rc) return rc;
+    int err = 0;
+    MLP_CUDA(cudaMemcpyAsync(out, st.target, (size_t)n * 4, cudaMemcpyDeviceToHost, m->stream));
+    MLP_CUDA(cudaMemcpyAsync(&err, m->tc_err, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+    MLP_CUDA(cudaStreamSynchronize(m->stream));
+    if (err) {
+        set_last_error("tensor-core MMA completion wait expired");
+        return NQ_ERR_TIMEOUT;
+    }
     return NQ_OK;
 }
 
@@ -721,9 +977,8 @@ int nq_schedule_device(nq_mlp *m, int N, const uint32_t *d_cols, const uint32_t 
     uint16_t *key2 = key + n;
     uint32_t *idx = (uint32_t *)(((uintptr_t)(key2 + n) + 15) & ~(uintptr_t)15);
     TaskView tv{d_cols, d_ld, d_rd, nullptr, nullptr, N};
-    const int grid = (int)std::min<long long>((n + kGroup - 1) / kGroup, (long long)m->sms * 8);
-    mlp_predict_kernel<<<grid, kH1, 0, s>>>(tv, n, m->w, pred);
-    MLP_CUDA(cudaGetLastError());
+    rc = launch_predict_tc(m, tv, n, pred, s);
+    if (rc) return rc;
     mlp_bin_kernel<<<m->sms * 4, 256, 0, s>>>(pred, n, key, idx);
     MLP_CUDA(cudaGetLastError());
     size_t tmp = 0;

@@ -47,6 +47,8 @@ def _declare():
     L.nq_mlp_set_params.argtypes = [_mlpp, _f32p]
     L.nq_mlp_predict.restype = ctypes.c_int
     L.nq_mlp_predict.argtypes = [_mlpp, ctypes.c_int, _u32p, _u32p, _u32p, ctypes.c_int64, _f32p]
+    L.nq_mlp_predict_tensor.restype = ctypes.c_int
+    L.nq_mlp_predict_tensor.argtypes = [_mlpp, ctypes.c_int, _u32p, _u32p, _u32p, ctypes.c_int64, _f32p]
     L.nq_mlp_grad.restype = ctypes.c_int
     L.nq_mlp_grad.argtypes = [_mlpp, _u8p, _u32p, _u32p, _u32p, _f32p, ctypes.c_int64, _f32p, _f32p]
     L.nq_mlp_train.restype = ctypes.c_int
@@ -102,6 +104,14 @@ class CostModel:
         out = np.empty(cols.size, np.float32)
         _check(lib.nq_mlp_predict(self._m, N, _p(cols, _u32p), _p(ld, _u32p), _p(rd, _u32p), cols.size,
                                   _p(out, _f32p)), "nq_mlp_predict")
+        return out
+
+    def predict_tensor(self, N: int, cols, ld, rd) -> np.ndarray:
+        """Forward on the tensor cores (tcgen05), as the scheduler runs it."""
+        cols, ld, rd = _u32(cols), _u32(ld), _u32(rd)
+        out = np.empty(cols.size, np.float32)
+        _check(lib.nq_mlp_predict_tensor(self._m, N, _p(cols, _u32p), _p(ld, _u32p), _p(rd, _u32p), cols.size,
+                                         _p(out, _f32p)), "nq_mlp_predict_tensor")
         return out
 
     def grad(self, task_n, cols, ld, rd, target):

@@ -54,10 +54,13 @@ def unpack(params: np.ndarray):
     return W1, b1, W2, b2, W3, b3
 
 
-def forward(params, X):
+def forward(params, X, h1_bf16: bool = False):
+    """Forward pass; h1_bf16 rounds the layer-1 outputs to BF16 (the tensor-core path's operand)."""
     W1, b1, W2, b2, W3, b3 = unpack(params)
     a1 = X @ W1.T + b1
     h1 = np.maximum(a1, 0)
+    if h1_bf16:
+        h1 = bf16_round(h1.astype(np.float32)).astype(np.float64)
     a2 = h1 @ W2.T + b2
     h2 = np.maximum(a2, 0)
     out = h2 @ W3 + b3

@@ -14,6 +14,11 @@ pytestmark = pytest.mark.gpu
 GRAD_RTOL_MAX = 2e-3      # max |g_gpu - g_ref| <= 2e-3 * max |g_ref|
 GRAD_RTOL_L2 = 2e-4       # ||g_gpu - g_ref|| <= 2e-4 * ||g_ref||
 PRED_ATOL = 2e-3          # |pred_gpu - pred_ref| for outputs of size ~10
+# Tensor-core forward: an FP32 layer-1 sum that lands next to a BF16 rounding
+# boundary may round the other way than the oracle's float64 sum (one BF16 ulp
+# of that activation), so the bound is looser than PRED_ATOL.
+TC_ATOL_MAX = 2e-2
+TC_ATOL_MEAN = 1e-3
 
 
 def _params(seed):
@@ -104,7 +109,27 @@ def test_schedule_is_a_longest_first_permutation(gpu):
     assert np.all(np.diff(keys) <= 0)                      # longest first
     same = np.diff(keys) == 0
     assert np.all(np.diff(o)[same] > 0)                    # stable inside a bin
-    assert np.allclose(pr, m.predict(16, c, l, r), atol=1e-5)
+    assert np.array_equal(pr, m.predict_tensor(16, c, l, r))   # the scheduler runs the tensor-core forward
+    m.close()
+
+
+def test_tensor_core_forward_matches_oracle(gpu):
+    # tcgen05 forward: BF16 operands (the layer-1 outputs rounded to BF16),
+    # FP32 accumulation in TMEM.  Against the oracle with the same rounding,
+    # and against the CUDA-core forward (which keeps layer 1 in FP32).
+    from n_queens_b200 import learned
+    m = learned.CostModel(seed=5)
+    for seed, (N, k) in ((4, (12, 4)), (8, (16, 5)), (9, (17, 6))):
+        p = _params(seed)
+        m.set_params(p)
+        c, l, r = oracle.expand(N, k)
+        sel = np.random.default_rng(seed).choice(c.size, min(5000, c.size), replace=False)
+        c, l, r = c[sel], l[sel], r[sel]
+        got = m.predict_tensor(N, c, l, r)
+        want, _ = mlp_ref.forward(p, mlp_ref.features(N, c, l, r), h1_bf16=True)
+        err = np.abs(got - want)
+        assert err.max() <= TC_ATOL_MAX and err.mean() <= TC_ATOL_MEAN, (err.max(), err.mean())
+        assert np.abs(got - m.predict(N, c, l, r)).max() <= 0.05
     m.close()
 
 
