@@ -296,6 +296,43 @@ int nq_schedule_device(nq_mlp *m, int N, const uint32_t *d_cols, const uint32_t 
  * prediction + sort time.  The model must live on cfg->device. */
 int nq_count_learned(int N, int rows, nq_mlp *m, const nq_config *cfg, uint64_t *total, nq_stats *stats);
 
+/* ---- Dihedral (8-fold) decomposition (no counterpart in the reference) ----
+ * The reference counts only the left-right mirror: row 0 in the left half,
+ * every prefix x2 (src/n_queens.cpp:74-113, src/n_queens_cuda.cu:181-183).
+ * These entries use all eight symmetries of the square: the tasks fall into
+ * classes (a corner queen; the border queen nearest a corner at distance m;
+ * all border queens at distance >= rows) whose searches follow the class's
+ * rules and whose completions carry the class's weights, so the weighted sum
+ * is the whole-board total with ~1.75x fewer DFS nodes than the reference's
+ * decomposition.  rows (the prefix depth) must be in [2, N-2], 4 <= N <= 31. */
+
+/* Rules of one class: rows beyond side_row may not use column 0 or N-1;
+ * row N-1 may use only last_mask's columns; a completion weighs weight_tie
+ * when its row N-1 queen is at tie_bit, else weight. */
+typedef struct {
+    int32_t side_row;
+    uint32_t last_mask;
+    uint32_t tie_bit;
+    uint32_t weight;
+    uint32_t weight_tie;
+} nq_dihedral_class;
+
+/* The task list of (N, rows) in host memory: cols (on-board bits), ld, rd as
+ * the reference packs prefixes, cls[i] the class index of task i.  Writes at
+ * most cap tasks (cap 0 and NULL arrays: count only) and at most cap_classes
+ * classes; *n_tasks and *n_classes receive the full counts.  Host only. */
+int nq_dihedral_expand(int N, int rows, uint32_t *cols, uint32_t *ld, uint32_t *rd, uint8_t *cls, int64_t cap,
+                       int64_t *n_tasks, nq_dihedral_class *classes, int cap_classes, int *n_classes);
+/* Whole-board total through the dihedral decomposition (the same total as
+ * nq_count / cuda_n_queens).  stats->tasks counts the dihedral tasks. */
+int nq_count_dihedral(int N, int rows, const nq_config *cfg, uint64_t *total, nq_stats *stats);
+/* Weighted counts of a caller's dihedral tasks (host arrays, the classes of
+ * (N, rows)): per_task[i] (optional) receives task i's weighted count, *sum
+ * their sum. */
+int nq_count_dihedral_tasks(int N, int rows, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd,
+                            const uint8_t *cls, int64_t n, uint64_t *per_task, uint64_t *sum, const nq_config *cfg,
+                            nq_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif

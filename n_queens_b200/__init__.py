@@ -108,6 +108,12 @@ class TuneEntry(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class DihedralClass(ctypes.Structure):
+    """``nq_dihedral_class``: the search rules and weights of one dihedral class."""
+    _fields_ = [("side_row", ctypes.c_int32), ("last_mask", ctypes.c_uint32), ("tie_bit", ctypes.c_uint32),
+                ("weight", ctypes.c_uint32), ("weight_tie", ctypes.c_uint32)]
+
+
 class Instance(ctypes.Structure):
     """Mirror of ``nq_instance``: one partial board."""
 
@@ -117,6 +123,7 @@ class Instance(ctypes.Structure):
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _i64p = ctypes.POINTER(ctypes.c_int64)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
 _cfgp = ctypes.POINTER(Config)
 _stp = ctypes.POINTER(Stats)
 
@@ -166,6 +173,14 @@ def _load() -> ctypes.CDLL:
                                     ctypes.POINTER(TuneEntry)]
     L.nq_count_batch.restype = ctypes.c_int
     L.nq_count_batch.argtypes = [ctypes.POINTER(Instance), ctypes.c_int64, ctypes.c_int, _u64p, _cfgp, _stp]
+    L.nq_dihedral_expand.restype = ctypes.c_int
+    L.nq_dihedral_expand.argtypes = [ctypes.c_int, ctypes.c_int, _u32p, _u32p, _u32p, _u8p, ctypes.c_int64, _i64p,
+                                     ctypes.POINTER(DihedralClass), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.nq_count_dihedral.restype = ctypes.c_int
+    L.nq_count_dihedral.argtypes = [ctypes.c_int, ctypes.c_int, _cfgp, _u64p, _stp]
+    L.nq_count_dihedral_tasks.restype = ctypes.c_int
+    L.nq_count_dihedral_tasks.argtypes = [ctypes.c_int, ctypes.c_int, _u32p, _u32p, _u32p, _u8p, ctypes.c_int64,
+                                          _u64p, _u64p, _cfgp, _stp]
     return L
 
 
@@ -178,7 +193,8 @@ EXPORTS = ("nq_abi_version", "nq_status_string", "nq_last_error", "nq_device_cou
            "nq_count_tasks", "nq_count_tasks_device", "nq_count_tasks_device_noalloc", "nq_count_batch",
            "nq_batch_create", "nq_batch_run", "nq_batch_destroy", "nq_batch_autotune",
            "nq_mlp_num_params", "nq_mlp_create", "nq_mlp_destroy", "nq_mlp_get_params", "nq_mlp_set_params",
-           "nq_mlp_predict", "nq_mlp_predict_tensor", "nq_mlp_grad", "nq_mlp_train", "nq_schedule_device", "nq_count_learned")
+           "nq_mlp_predict", "nq_mlp_predict_tensor", "nq_mlp_grad", "nq_mlp_train", "nq_schedule_device", "nq_count_learned",
+           "nq_dihedral_expand", "nq_count_dihedral", "nq_count_dihedral_tasks")
 
 
 def status_string(status: int) -> str:
@@ -249,6 +265,52 @@ def count(N: int, rows: int, config=None, nodes: bool = False) -> CountResult:
                       ctypes.byref(st))
     _check(rc, "nq_count")
     return CountResult(int(tot.value), int(nd.value) if nodes else None, st.as_dict())
+
+
+def dihedral_expand(N: int, rows: int):
+    """Dihedral (8-fold) task list of (N, rows) (``nq_dihedral_expand``).
+
+    Returns ``(cols, ld, rd, cls, classes)``: uint32 arrays, the uint8 class
+    index per task, and the class table as a list of dicts.
+    """
+    n = ctypes.c_int64(0)
+    ncls = ctypes.c_int(0)
+    _check(lib.nq_dihedral_expand(N, rows, None, None, None, None, 0, ctypes.byref(n), None, 0, ctypes.byref(ncls)),
+           "nq_dihedral_expand")
+    c, l, r = (np.empty(n.value, np.uint32) for _ in range(3))
+    k = np.empty(n.value, np.uint8)
+    tab = (DihedralClass * max(ncls.value, 1))()
+    _check(lib.nq_dihedral_expand(N, rows, _p(c, _u32p), _p(l, _u32p), _p(r, _u32p), _p(k, _u8p), n.value,
+                                  ctypes.byref(n), tab, ncls.value, ctypes.byref(ncls)), "nq_dihedral_expand")
+    classes = [{f: getattr(tab[i], f) for f, _ in DihedralClass._fields_} for i in range(ncls.value)]
+    return c, l, r, k, classes
+
+
+def count_dihedral(N: int, rows: int, config=None) -> CountResult:
+    """Whole-board count through the dihedral decomposition (``nq_count_dihedral``)."""
+    tot = ctypes.c_uint64(0)
+    st = Stats()
+    rc = lib.nq_count_dihedral(N, rows, _cfg(config), ctypes.byref(tot), ctypes.byref(st))
+    _check(rc, "nq_count_dihedral")
+    return CountResult(int(tot.value), None, st.as_dict())
+
+
+def count_dihedral_tasks(N: int, rows: int, cols, ld, rd, cls, per_task: bool = False, config=None) -> dict:
+    """Weighted counts of dihedral tasks (``nq_count_dihedral_tasks``)."""
+    cols = np.ascontiguousarray(cols, np.uint32)
+    ld = np.ascontiguousarray(ld, np.uint32)
+    rd = np.ascontiguousarray(rd, np.uint32)
+    cls = np.ascontiguousarray(cls, np.uint8)
+    n = cols.size
+    if ld.size != n or rd.size != n or cls.size != n:
+        raise ValueError("cols, ld, rd and cls must have the same length")
+    pt = np.empty(n, np.uint64) if per_task else None
+    s = ctypes.c_uint64(0)
+    st = Stats()
+    rc = lib.nq_count_dihedral_tasks(N, rows, _p(cols, _u32p), _p(ld, _u32p), _p(rd, _u32p), _p(cls, _u8p), n,
+                                     _p(pt, _u64p), ctypes.byref(s), _cfg(config), ctypes.byref(st))
+    _check(rc, "nq_count_dihedral_tasks")
+    return {"sum": int(s.value), "per_task": pt, "stats": st.as_dict()}
 
 
 def count_resumable(N: int, rows: int, checkpoint: str, slice_ms: int = 0, config=None):

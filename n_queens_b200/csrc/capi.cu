@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "dfs_kernel.cuh"
+#include "dihedral.h"
 #include "expand.h"
 #include "n_queens_b200.h"
 
@@ -86,7 +87,8 @@ KernelFn pick_variant(int v) {
     }
 }
 
-KernelFn pick_kernel(bool per_owner, bool nodes, int v = -1) {
+KernelFn pick_kernel(bool per_owner, bool nodes, int v = -1, bool dih = false) {
+    if (dih) return per_owner ? dfs_kernel<true, false, 1, 8, false, true> : dfs_kernel<false, false, 1, 8, false, true>;
     if (v < 0) v = step_variant();
     if (per_owner) return nodes ? pick_variant<true, true>(v) : pick_variant<true, false>(v);
     return nodes ? pick_variant<false, true>(v) : pick_variant<false, false>(v);
@@ -171,6 +173,9 @@ int ensure_ready(Ctx &c, int dev) {
                                              c.smem_optin - static_smem));
     NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, 1, 8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  c.smem_optin - static_smem));
+    for (int po = 0; po < 2; ++po)
+        NQ_CUDA(cudaFuncSetAttribute(pick_kernel(po, false, -1, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     c.smem_optin - static_smem));
     c.ready = true;
     return NQ_OK;
 }
@@ -195,11 +200,14 @@ int lock_device(int dev, Ctx *&out) {
 
 struct Launch {
     int threads = 0, levels = 0, smem = 0, grid = 0, inner = 0, steal = 1, layout = 0;
+    bool dih = false;  // dihedral-decomposition kernel
 };
 
 // Chooses the persistent grid: CTA size, stack slots per lane and as many
 // resident CTAs per SM as shared memory and registers allow.
-int plan_launch(Ctx &c, const nq_config *cfg, int levels_needed, bool per_owner, bool nodes, Launch &L) {
+int plan_launch(Ctx &c, const nq_config *cfg, int levels_needed, bool per_owner, bool nodes, Launch &L,
+                bool dih = false) {
+    L.dih = dih;
     L.threads = (cfg && cfg->block_threads) ? cfg->block_threads : kDefaultThreads;
     if (L.threads < 32 || L.threads > 1024 || (L.threads & 31)) {
         g_last_error = "block_threads must be a multiple of 32 in [32, 1024]";
@@ -220,8 +228,8 @@ int plan_launch(Ctx &c, const nq_config *cfg, int levels_needed, bool per_owner,
         return NQ_ERR_DEPTH;
     }
     int per_sm = 0;
-    NQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_kernel(per_owner, nodes), L.threads,
-                                                          L.smem));
+    NQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_kernel(per_owner, nodes, -1, dih),
+                                                          L.threads, L.smem));
     if (per_sm <= 0) {
         g_last_error = "launch configuration cannot be resident";
         return NQ_ERR_ARG;
@@ -251,7 +259,7 @@ int enqueue_dfs(Ctx &c, DfsParams p, const Launch &L, bool per_owner, bool nodes
     p.layout = L.layout;
     NQ_CUDA(cudaMemsetAsync(p.ctl, 0, kCtlWords * sizeof(unsigned long long), s));
     if (p.cta_times) NQ_CUDA(cudaMemsetAsync(p.cta_times, 0, 2 * (size_t)L.grid * sizeof(unsigned long long), s));
-    pick_kernel(per_owner, nodes)<<<L.grid, L.threads, L.smem, s>>>(p);
+    pick_kernel(per_owner, nodes, -1, L.dih)<<<L.grid, L.threads, L.smem, s>>>(p);
     NQ_CUDA(cudaGetLastError());
     return NQ_OK;
 }
@@ -318,18 +326,31 @@ int timing_stats(const unsigned long long *d_times, int grid, nq_stats *st) {
 
 // Counts tasks that are already in device memory (d_cols, d_ld, d_rd) and
 // downloads the results.  Used by nq_count and nq_count_tasks.
+// Class data of a dihedral launch (device pointers).
+struct DihArgs {
+    const uint8_t *task_cls = nullptr;
+    const uint4 *cls_tab = nullptr;
+    uint32_t noside = 0;
+};
+
 int count_resident(Ctx &c, int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd, int64_t n,
                    int levels_needed, const nq_config *cfg, bool per_owner, bool nodes, uint64_t *h_per_task,
                    uint64_t *h_nodes_task, uint64_t *sum, uint64_t *nodes_total, nq_stats *st, bool timed_h2d,
-                   const uint32_t *d_order = nullptr) {
+                   const uint32_t *d_order = nullptr, const DihArgs *dih = nullptr) {
+    if (dih) nodes = false;
     Launch L;
-    int rc = plan_launch(c, cfg, levels_needed, per_owner, nodes, L);
+    int rc = plan_launch(c, cfg, levels_needed, per_owner, nodes, L, dih != nullptr);
     if (rc) return rc;
     fill_stats_launch(st, L);
     DfsParams p = base_params(c, N, n, cfg);
     p.cols = d_cols;
     p.ld = d_ld;
     p.rd = d_rd;
+    if (dih) {
+        p.task_cls = dih->task_cls;
+        p.cls_tab = dih->cls_tab;
+        p.noside = dih->noside;
+    }
     // aux layout: [order u32 n] [out_cnt u64 n] [out_nodes u64 n]
     size_t off_order = 0, off_cnt = 0, off_nodes = 0, need = 0;
     const bool given = !d_order && cfg && cfg->order_kind == NQ_ORDER_GIVEN && cfg->order;
@@ -1209,6 +1230,129 @@ int nq_batch_autotune(const nq_instance *inst, int64_t n, int repeats, const nq_
             }
     if (n_entries) *n_entries = count;
     return best->ms < 0 ? NQ_ERR_ARG : NQ_OK;
+}
+
+int nq_dihedral_expand(int N, int rows, uint32_t *cols, uint32_t *ld, uint32_t *rd, uint8_t *cls, int64_t cap,
+                       int64_t *n_tasks, nq_dihedral_class *classes, int cap_classes, int *n_classes) {
+    std::vector<DihClass> tab;
+    if (!dihedral_classes(N, rows, tab) || cap < 0 || cap_classes < 0) return NQ_ERR_ARG;
+    if (cap > 0 && (!cols || !ld || !rd || !cls)) return NQ_ERR_ARG;
+    static_assert(sizeof(DihClass) == sizeof(nq_dihedral_class), "class layout");
+    if (classes)
+        for (int i = 0; i < (int)tab.size() && i < cap_classes; ++i) memcpy(&classes[i], &tab[i], sizeof(DihClass));
+    if (n_classes) *n_classes = (int)tab.size();
+    const int64_t n = dihedral_expand(N, rows, cols, ld, rd, cls, cap);
+    if (n < 0) return NQ_ERR_ARG;
+    if (n_tasks) *n_tasks = n;
+    return NQ_OK;
+}
+
+namespace {
+
+// Uploads the class table of (N, rows) behind `used` bytes of c.tasks and
+// fills the launch's class arguments.  The caller has grown c.tasks.
+int dih_upload_classes(Ctx &c, int N, int rows, size_t used, DihArgs &a) {
+    std::vector<DihClass> tab;
+    if (!dihedral_classes(N, rows, tab) || tab.size() > (size_t)kMaxDihClasses) return NQ_ERR_ARG;
+    uint4 h[kMaxDihClasses];  // synchronous copy below: the array may go out of scope after it
+    for (size_t i = 0; i < tab.size(); ++i) {
+        const DihClass &t = tab[i];
+        // popc of a child's column mask (off-board bits set) is 32 - N + its
+        // row; rows beyond side_row are popc values beyond this threshold.
+        const int thr = 32 - N + t.side_row;
+        h[i] = make_uint4((uint32_t)std::min(thr, 64), t.last_mask, t.tie_bit, t.w | (t.w_tie << 16));
+    }
+    const size_t off = (used + 255) & ~(size_t)255;
+    uint4 *d = (uint4 *)((char *)c.tasks.p + off);
+    NQ_CUDA(cudaMemcpy(d, h, tab.size() * sizeof(uint4), cudaMemcpyHostToDevice));
+    a.cls_tab = d;
+    a.noside = ~(1u | (1u << (N - 1)));
+    return NQ_OK;
+}
+
+size_t dih_bytes(int64_t n) {
+    return (((size_t)std::max<int64_t>(n, 1) * 13 + 255) & ~(size_t)255) + kMaxDihClasses * sizeof(uint4);
+}
+
+}  // namespace
+
+int nq_count_dihedral(int N, int rows, const nq_config *cfg, uint64_t *total, nq_stats *stats) {
+    const double t0 = now_ms();
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (!total || N < 4 || N > NQ_MAX_N || rows < 2 || rows > N - 2) return NQ_ERR_ARG;
+    Ctx *cp = nullptr;
+    int rc = lock_device(device_of(cfg), cp);
+    if (rc) return rc;
+    Ctx &c = *cp;
+    std::lock_guard<std::mutex> lock(c.mu);
+    rc = ensure_ready(c, device_of(cfg));
+    if (rc) return rc;
+    const double te = now_ms();
+    const int64_t n = dihedral_expand(N, rows, nullptr, nullptr, nullptr, nullptr, 0);
+    if (n < 0 || n > 0xffffffffll) return NQ_ERR_ARG;
+    // host staging: cols | ld | rd (u32) | cls (u8)
+    rc = c.h_tasks.grow((size_t)std::max<int64_t>(n, 1) * 13);
+    if (rc) return rc;
+    uint32_t *h = (uint32_t *)c.h_tasks.p;
+    uint8_t *hc = (uint8_t *)(h + 3 * n);
+    dihedral_expand(N, rows, h, h + n, h + 2 * n, hc, n);
+    if (stats) {
+        stats->expand_ms = now_ms() - te;
+        stats->tasks = n;
+    }
+    rc = c.tasks.grow(dih_bytes(n));
+    if (rc) return rc;
+    uint32_t *d = (uint32_t *)c.tasks.p;
+    DihArgs a;
+    a.task_cls = (const uint8_t *)(d + 3 * n);
+    rc = dih_upload_classes(c, N, rows, (size_t)n * 13, a);
+    if (rc) return rc;
+    NQ_CUDA(cudaEventRecord(c.ev[0], c.stream));
+    if (n) NQ_CUDA(cudaMemcpyAsync(d, h, (size_t)n * 13, cudaMemcpyHostToDevice, c.stream));
+    uint64_t sum = 0;
+    rc = count_resident(c, N, d, d + n, d + 2 * n, n, N - 1 - rows, cfg, false, false, nullptr, nullptr, &sum,
+                        nullptr, stats, true, nullptr, &a);
+    *total = sum;  // the class weights already carry every symmetry factor
+    if (stats) stats->total_ms = now_ms() - t0;
+    return rc;
+}
+
+int nq_count_dihedral_tasks(int N, int rows, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd,
+                            const uint8_t *cls, int64_t n, uint64_t *per_task, uint64_t *sum, const nq_config *cfg,
+                            nq_stats *stats) {
+    const double t0 = now_ms();
+    if (stats) memset(stats, 0, sizeof(*stats));
+    std::vector<DihClass> tab;
+    if (!sum || n < 0 || n > 0xffffffffll || !dihedral_classes(N, rows, tab)) return NQ_ERR_ARG;
+    if (n > 0 && (!cols || !ld || !rd || !cls)) return NQ_ERR_ARG;
+    for (int64_t i = 0; i < n; ++i)
+        if (cls[i] >= tab.size()) return NQ_ERR_ARG;
+    *sum = 0;
+    if (n == 0) return NQ_OK;
+    Ctx *cp = nullptr;
+    int rc = lock_device(device_of(cfg), cp);
+    if (rc) return rc;
+    Ctx &c = *cp;
+    std::lock_guard<std::mutex> lock(c.mu);
+    rc = ensure_ready(c, device_of(cfg));
+    if (rc) return rc;
+    rc = c.tasks.grow(dih_bytes(n));
+    if (rc) return rc;
+    uint32_t *d = (uint32_t *)c.tasks.p;
+    DihArgs a;
+    a.task_cls = (const uint8_t *)(d + 3 * n);
+    rc = dih_upload_classes(c, N, rows, (size_t)n * 13, a);
+    if (rc) return rc;
+    NQ_CUDA(cudaEventRecord(c.ev[0], c.stream));
+    NQ_CUDA(cudaMemcpyAsync(d, cols, (size_t)n * 4, cudaMemcpyHostToDevice, c.stream));
+    NQ_CUDA(cudaMemcpyAsync(d + n, ld, (size_t)n * 4, cudaMemcpyHostToDevice, c.stream));
+    NQ_CUDA(cudaMemcpyAsync(d + 2 * n, rd, (size_t)n * 4, cudaMemcpyHostToDevice, c.stream));
+    NQ_CUDA(cudaMemcpyAsync(d + 3 * n, cls, (size_t)n, cudaMemcpyHostToDevice, c.stream));
+    const int need = levels_for_tasks(N, cols, n);
+    rc = count_resident(c, N, d, d + n, d + 2 * n, n, need, cfg, per_task != nullptr, false, per_task, nullptr, sum,
+                        nullptr, stats, true, nullptr, &a);
+    if (stats) stats->total_ms = now_ms() - t0;
+    return rc;
 }
 
 int nq_count_batch(const nq_instance *inst, int64_t n, int split_rows, uint64_t *out, const nq_config *cfg,

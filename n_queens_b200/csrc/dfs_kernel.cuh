@@ -90,6 +90,13 @@ struct DfsParams {
     uint4 *cont_out;
     uint32_t *cont_out_owner;        // optional
     long long cont_cap;
+    // Dihedral decomposition (DIH kernels only): class index per task and the
+    // class table {popc threshold, row N-1 mask, tie column bit,
+    // weight | tie weight << 16}; a child whose column mask (off-board bits
+    // set) has more bits than the threshold may not use column 0 or N-1.
+    const uint8_t *task_cls;
+    const uint4 *cls_tab;
+    uint32_t noside;                 // ~(column 0 | column N-1)
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -195,6 +202,45 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"                                \
     "}\n\t"
 
+// Dihedral step: the VAR 1 step plus the class rules of the lane's task.
+//   pc = popc(child cols) = 32 - N + child row
+//   pc > %12            -> the child row may not use the side columns, and
+//                          when it is row N-1 (pc == 31) only %13's columns
+//   child cols == ~0    -> one completion of weight %16 if the row N-1 queen
+//                          is at %14, else %15
+// Operands %0-%11 as in the plain step; %12 popc threshold, %13 row N-1
+// mask, %14 tie column bit, %15 weight, %16 tie weight, %17 ~side columns.
+#define NQB_STEP_HEAD_DIH                                                             \
+    "{\n\t"                                                                           \
+    ".reg .pred pb, pd, pp, pe, pq, ps, pl, px;\n\t"                                  \
+    ".reg .b32 t, bit, nc, nl, nr, na, pc, msk, w;\n\t"
+
+#define NQB_STEP_CHILD_DIH                                                            \
+    "mul.lo.s32 t, %3, %10;\n\t"                                                      \
+    "and.b32 bit, t, %3;\n\t"                                                         \
+    "setp.ne.u32 pb, bit, 0;\n\t"                                                     \
+    "mad.lo.s32 %3, bit, %10, %3;\n\t"                                                \
+    "mad.lo.s32 nc, bit, %8, %0;\n\t"                                                 \
+    "or.b32 nl, %1, bit;\n\t"                                                         \
+    "mul.lo.s32 nl, nl, %9;\n\t"                                                      \
+    "or.b32 nr, %2, bit;\n\t"                                                         \
+    "shr.s32 nr, nr, 1;\n\t"                                                          \
+    "lop3.b32 na, nc, nl, nr, 0x01;\n\t"                                              \
+    "popc.b32 pc, nc;\n\t"                                                            \
+    "setp.gt.u32 ps, pc, %12;\n\t"                                                    \
+    "setp.eq.u32 pl, pc, 31;\n\t"                                                     \
+    "selp.b32 msk, %13, %17, pl;\n\t"                                                 \
+    "@ps and.b32 na, na, msk;\n\t"                                                    \
+    "setp.eq.u32 pe, nc, 0xffffffff;\n\t"                                             \
+    "setp.eq.u32 px, bit, %14;\n\t"                                                   \
+    "selp.b32 w, %16, %15, px;\n\t"                                                   \
+    "@pe add.u32 %5, %5, w;\n\t"
+
+// Class registers of a lane in a DIH kernel.
+struct DihLane {
+    uint32_t side_popc = 64u, last_mask = ~0u, tie_bit = 0u, w = 0u, w_tie = 0u;
+};
+
 struct StepConsts {
     uint32_t one, two, mone, stride;  // stride: bytes between a lane's consecutive stack slots
 };
@@ -218,6 +264,25 @@ __device__ __forceinline__ void dfs_step(uint32_t &cols, uint32_t &ld, uint32_t 
             asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR1 NQB_STEP_TAIL_VAR1 NQB_STEP_OPERANDS);
     }
 #undef NQB_STEP_OPERANDS
+}
+
+__device__ __forceinline__ void dfs_step_dih(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail, uint32_t &sp,
+                                             uint32_t &cnt, uint32_t &it, uint32_t bot, const StepConsts &k,
+                                             const DihLane &d, uint32_t noside) {
+    asm volatile(NQB_STEP_HEAD_DIH NQB_STEP_CHILD_DIH NQB_STEP_TAIL_VAR1
+                 : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
+                 : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(d.side_popc), "r"(d.last_mask),
+                   "r"(d.tie_bit), "r"(d.w), "r"(d.w_tie), "r"(noside)
+                 : "memory");
+}
+
+__device__ __forceinline__ void load_class(const DfsParams &p, long long t, DihLane &d) {
+    const uint4 c = __ldg(p.cls_tab + __ldg(p.task_cls + t));
+    d.side_popc = c.x;
+    d.last_mask = c.y;
+    d.tie_bit = c.z;
+    d.w = c.w & 0xffffu;
+    d.w_tie = c.w >> 16;
 }
 
 // Loads task t into a lane.  Returns the completions credited immediately
@@ -251,7 +316,9 @@ __device__ __forceinline__ uint32_t load_task(const DfsParams &p, long long t, u
 // RESUME adds the continuation queue and the deadline dump; it is a separate
 // instantiation so that the plain count kernel carries none of that code
 // (it measurably changed the code generated for the DFS loop).
-template <bool PER_OWNER, bool NODES, int VAR, int UNROLL, bool RESUME = false>
+// DIH runs the dihedral decomposition: every task carries a class (rules and
+// weights, see DfsParams::cls_tab) and the step is dfs_step_dih.
+template <bool PER_OWNER, bool NODES, int VAR, int UNROLL, bool RESUME = false, bool DIH = false>
 __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long red_cnt[32];
@@ -275,6 +342,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
     uint32_t sp = my_base, bot = my_base;
     uint32_t cnt = 0, it = 0;
     uint32_t owner = kNoOwner;
+    DihLane dih;
     unsigned long long tot = 0, tot_nodes = 0;
     const long long qlen = RESUME ? p.n_cont_in + p.ntasks - p.task_base : p.ntasks;
     bool queue_live = qlen > 0;
@@ -351,7 +419,11 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                         // A permutation entry out of range is skipped, never dereferenced.
                         if (t >= 0 && t < p.ntasks) {
                             sp = bot = my_base;
-                            const uint32_t done = load_task(p, t, cols, ld, rd, avail);
+                            uint32_t done = load_task(p, t, cols, ld, rd, avail);
+                            if (DIH) {
+                                load_class(p, t, dih);
+                                done *= dih.w;
+                            }
                             const uint32_t own = p.owner_of ? __ldg(p.owner_of + t) : (uint32_t)t;
                             if (PER_OWNER) {
                                 if (done) atomicAdd(p.out_cnt + own, (unsigned long long)done);
@@ -384,10 +456,20 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                         }
                         const uint32_t src_addr = __shfl_sync(kFull, bot, donor < 0 ? lane : donor);
                         const uint32_t src_owner = __shfl_sync(kFull, owner, donor < 0 ? lane : donor);
+                        DihLane src_dih;
+                        if (DIH) {
+                            const int src = donor < 0 ? (int)lane : donor;
+                            src_dih.side_popc = __shfl_sync(kFull, dih.side_popc, src);
+                            src_dih.last_mask = __shfl_sync(kFull, dih.last_mask, src);
+                            src_dih.tie_bit = __shfl_sync(kFull, dih.tie_bit, src);
+                            src_dih.w = __shfl_sync(kFull, dih.w, src);
+                            src_dih.w_tie = __shfl_sync(kFull, dih.w_tie, src);
+                        }
                         if (donor >= 0) {
                             lds128(src_addr, cols, ld, rd, avail);
                             sp = bot = my_base;
                             owner = src_owner;
+                            if (DIH) dih = src_dih;
                         }
                         __syncwarp();
                         if (sp != bot && __popc(rich & lanemask_lt()) < npair) bot += stride;
@@ -409,13 +491,23 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
         if (check_idle) {
             for (int s = 0; s < p.inner; s += UNROLL) {
 #pragma unroll
-                for (int u = 0; u < UNROLL; ++u) dfs_step<NODES, VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
+                for (int u = 0; u < UNROLL; ++u) {
+                    if (DIH)
+                        dfs_step_dih(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
+                    else
+                        dfs_step<NODES, VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
+                }
                 if (__any_sync(kFull, avail == 0)) break;
             }
         } else {
             for (int s = 0; s < p.inner; s += UNROLL) {
 #pragma unroll
-                for (int u = 0; u < UNROLL; ++u) dfs_step<NODES, VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
+                for (int u = 0; u < UNROLL; ++u) {
+                    if (DIH)
+                        dfs_step_dih(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
+                    else
+                        dfs_step<NODES, VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
+                }
                 if (__all_sync(kFull, avail == 0)) break;
             }
         }

@@ -103,6 +103,61 @@ def total(N: int, rows: int, threads: int = 0, with_nodes: bool = False):
     return (int(s), int(nd.value)) if with_nodes else int(s)
 
 
+class DihClass(ctypes.Structure):
+    _fields_ = [("side_row", ctypes.c_int32), ("last_mask", ctypes.c_uint32), ("tie_bit", ctypes.c_uint32),
+                ("w", ctypes.c_uint32), ("w_tie", ctypes.c_uint32)]
+
+
+lib.nq_oracle_dihedral_expand.restype = ctypes.c_int64
+lib.nq_oracle_dihedral_expand.argtypes = [ctypes.c_int, ctypes.c_int, _u32p, _u32p, _u32p,
+                                          ctypes.POINTER(ctypes.c_uint8), ctypes.c_int64, ctypes.POINTER(DihClass),
+                                          ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+lib.nq_oracle_dihedral_count_tasks.restype = None
+lib.nq_oracle_dihedral_count_tasks.argtypes = [ctypes.c_int, ctypes.c_int64, _u32p, _u32p, _u32p,
+                                               ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(DihClass), _u64p,
+                                               ctypes.c_int]
+lib.nq_oracle_dihedral_total.restype = ctypes.c_int64
+lib.nq_oracle_dihedral_total.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+
+
+def dihedral_expand(N: int, rows: int):
+    """Dihedral decomposition tasks (dihedral_oracle.c): (cols, ld, rd, cls, classes as tuples)."""
+    ncls = ctypes.c_int(0)
+    n = lib.nq_oracle_dihedral_expand(N, rows, None, None, None, None, 0, None, 0, ctypes.byref(ncls))
+    if n < 0:
+        raise ValueError(f"bad (N, rows) = ({N}, {rows})")
+    c, l, r = (np.empty(n, np.uint32) for _ in range(3))
+    k = np.empty(n, np.uint8)
+    tab = (DihClass * 64)()
+    lib.nq_oracle_dihedral_expand(N, rows, _p(c, _u32p), _p(l, _u32p), _p(r, _u32p),
+                                  k.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), n, tab, 64, ctypes.byref(ncls))
+    classes = [(t.side_row, t.last_mask, t.tie_bit, t.w, t.w_tie) for t in tab[:ncls.value]]
+    return c, l, r, k, classes
+
+
+def dihedral_count_tasks(N: int, rows: int, cols, ld, rd, cls, threads: int = 0) -> np.ndarray:
+    """Weighted count of each dihedral task under its class's rules (OpenMP)."""
+    ncls = ctypes.c_int(0)
+    tab = (DihClass * 64)()
+    lib.nq_oracle_dihedral_expand(N, rows, None, None, None, None, 0, tab, 64, ctypes.byref(ncls))
+    cols = np.ascontiguousarray(cols, np.uint32)
+    ld = np.ascontiguousarray(ld, np.uint32)
+    rd = np.ascontiguousarray(rd, np.uint32)
+    cls = np.ascontiguousarray(cls, np.uint8)
+    if cls.size and int(cls.max()) >= ncls.value:
+        raise ValueError("class index out of range")
+    out = np.empty(cols.size, np.uint64)
+    lib.nq_oracle_dihedral_count_tasks(N, cols.size, _p(cols, _u32p), _p(ld, _u32p), _p(rd, _u32p),
+                                       cls.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), tab, _p(out, _u64p),
+                                       threads)
+    return out
+
+
+def dihedral_total(N: int, rows: int, threads: int = 0) -> int:
+    """Whole-board total through the dihedral decomposition."""
+    return int(lib.nq_oracle_dihedral_total(N, rows, threads))
+
+
 _ref_lib = None
 
 

@@ -1,0 +1,64 @@
+"""Dihedral (8-fold) decomposition: the oracle against known totals, and the
+library's host expander against the oracle's (no GPU needed).
+
+The decomposition has no counterpart in the reference; its only contract is
+the reference's whole-board total (README.md:16-25, logs/5090.log), which the
+oracle's plain total is pinned to in test_oracle.py.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import n_queens_b200 as nq
+import oracle
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _known(N):
+    pub = json.load(open(os.path.join(GOLDEN, "published.json")))
+    if str(N) in pub:
+        return pub[str(N)]["total"]
+    return oracle.total(N, 2 if N >= 4 else 1)
+
+
+@pytest.mark.parametrize("N", range(4, 15))
+def test_oracle_dihedral_total_every_depth(N):
+    want = _known(N)
+    for k in range(2, N - 1):
+        assert oracle.dihedral_total(N, k) == want, (N, k)
+
+
+@pytest.mark.parametrize("N,k", [(15, 4), (15, 5), (16, 5), (16, 6), (17, 6)])
+def test_oracle_dihedral_total_larger(N, k):
+    assert oracle.dihedral_total(N, k) == _known(N)
+
+
+@pytest.mark.parametrize("N,k", [(4, 2), (5, 3), (8, 3), (9, 4), (12, 5), (13, 6), (16, 5), (19, 6), (21, 6),
+                                 (22, 7)])
+def test_host_expander_matches_oracle(N, k):
+    c, l, r, cls, classes = nq.dihedral_expand(N, k)
+    oc, ol, orr, ocls, ocl = oracle.dihedral_expand(N, k)
+    assert c.size == oc.size
+    assert np.array_equal(c, oc) and np.array_equal(l, ol) and np.array_equal(r, orr)
+    assert np.array_equal(cls, ocls)
+    assert [(x["side_row"], x["last_mask"], x["tie_bit"], x["weight"], x["weight_tie"]) for x in classes] == ocl
+
+
+def test_dihedral_task_counts():
+    # 1.75x fewer DFS nodes needs no more tasks than the mirror decomposition
+    # at the same depth by more than a small factor.
+    for N, k in ((16, 5), (21, 6)):
+        n_dih = nq.dihedral_expand(N, k)[0].size
+        n_ref = nq.expand(N, k)[0].size
+        assert 0.3 * n_ref < n_dih < 1.2 * n_ref, (N, k, n_dih, n_ref)
+
+
+@pytest.mark.parametrize("N,k", [(3, 1), (4, 1), (4, 3), (8, 7), (32, 6), (10, 0)])
+def test_dihedral_rejects_bad_arguments(N, k):
+    with pytest.raises(nq.NQError):
+        nq.dihedral_expand(N, k)
+    with pytest.raises(nq.NQError):
+        nq.count_dihedral(N, k)

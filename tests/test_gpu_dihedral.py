@@ -1,0 +1,77 @@
+"""GPU parity of the dihedral (8-fold) decomposition, through the C ABI.
+
+Whole-board totals must equal the reference's (published totals, and the
+oracle's plain total, which test_oracle.py pins to the reference); per-task
+weighted counts must equal the oracle's restatement (oracle/dihedral_oracle.c)
+bit for bit.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+PUBLISHED = {int(k): v["total"] for k, v in json.load(open(os.path.join(GOLDEN, "published.json"))).items()}
+
+
+def _known(N):
+    return PUBLISHED[N] if N in PUBLISHED else oracle.total(N, 2)
+
+
+def test_whole_board_small_n_every_depth(gpu):
+    for N in range(4, 15):
+        want = _known(N)
+        for k in range(2, N - 1):
+            r = gpu.count_dihedral(N, k)
+            assert r.total == want, (N, k, r.total, want)
+
+
+@pytest.mark.parametrize("N,k", [(15, 5), (16, 4), (16, 6), (17, 6), (18, 6), (19, 5), (19, 6), (20, 6), (20, 7)])
+def test_whole_board_published(gpu, N, k):
+    r = gpu.count_dihedral(N, k)
+    assert r.total == PUBLISHED[N]
+    assert r.stats["tasks"] == gpu.dihedral_expand(N, k)[0].size
+
+
+@pytest.mark.parametrize("N,k", [(10, 3), (12, 4), (13, 5), (14, 5), (15, 5), (16, 6)])
+def test_per_task_matches_oracle(gpu, N, k):
+    c, l, r, cls, _ = gpu.dihedral_expand(N, k)
+    got = gpu.count_dihedral_tasks(N, k, c, l, r, cls, per_task=True)
+    want = oracle.dihedral_count_tasks(N, k, c, l, r, cls)
+    assert np.array_equal(got["per_task"], want)
+    assert got["sum"] == int(want.sum()) == _known(N)
+
+
+def test_shuffled_mixed_classes(gpu):
+    # Tasks of every class interleaved in the queue: lanes switch classes on
+    # each refill, and in-warp donation hands class rules across lanes.
+    N, k = 15, 5
+    c, l, r, cls, _ = gpu.dihedral_expand(N, k)
+    perm = np.random.default_rng(3).permutation(c.size)
+    c, l, r, cls = c[perm], l[perm], r[perm], cls[perm]
+    got = gpu.count_dihedral_tasks(N, k, c, l, r, cls, per_task=True,
+                                   config={"block_threads": 64, "inner_steps": 8})
+    want = oracle.dihedral_count_tasks(N, k, c, l, r, cls)
+    assert np.array_equal(got["per_task"], want)
+    # without donation, same result
+    got2 = gpu.count_dihedral_tasks(N, k, c, l, r, cls, config={"steal": -1})
+    assert got2["sum"] == _known(N)
+
+
+def test_time_limit_reports_timeout(gpu):
+    with pytest.raises(gpu.NQError) as e:
+        gpu.count_dihedral(21, 6, config={"time_limit_ms": 2})
+    assert e.value.status == gpu.NQ_ERR_TIMEOUT
+
+
+def test_rejects_class_index_out_of_range(gpu):
+    c, l, r, cls, classes = gpu.dihedral_expand(12, 4)
+    bad = cls.copy()
+    bad[0] = len(classes)
+    with pytest.raises(gpu.NQError):
+        gpu.count_dihedral_tasks(12, 4, c, l, r, bad)
