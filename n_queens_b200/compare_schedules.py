@@ -2,13 +2,14 @@
 expander order, on one GPU (the comparison the cost model exists for).
 
     python -m n_queens_b200.compare_schedules --N 22 --k 6 [--repeats 1] [--json out.json]
-                                              [--schedules plain,learned]
+                                              [--schedules plain,learned,dihedral]
 
 Builds the cost model once (solver-logged node counts at N=16..18, fine-tuned
 on a seeded 5% sample of the target's prefixes), then alternates plain and
 learned whole-board counts through the public API (nq_count and
 nq_count_learned), each with per-CTA timing, and prints wall time, kernel
-time, makespan, tail-idle fraction and the count of every run.
+time, makespan, tail-idle fraction and the count of every run.  `dihedral`
+adds the 8-fold decomposition (nq_count_dihedral) to the same alternation.
 """
 from __future__ import annotations
 
@@ -16,7 +17,7 @@ import argparse
 import json
 import time
 
-from . import count
+from . import count, count_dihedral
 from . import learned
 
 
@@ -27,7 +28,7 @@ def main():
     ap.add_argument("--repeats", type=int, default=1)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--json", default=None)
-    ap.add_argument("--schedules", default="plain,learned", help="comma list of plain, learned")
+    ap.add_argument("--schedules", default="plain,learned", help="comma list of plain, learned, dihedral")
     args = ap.parse_args()
     names = [x for x in args.schedules.split(",") if x]
     out = {"N": args.N, "k": args.k, "runs": []}
@@ -43,13 +44,15 @@ def main():
             t = time.perf_counter()
             if name == "plain":
                 r = count(args.N, args.k, config=dict(timing=1))
+            elif name == "dihedral":
+                r = count_dihedral(args.N, args.k, config=dict(timing=1))
             else:
                 r = learned.count_learned(args.N, args.k, model, config=dict(timing=1))
             wall = time.perf_counter() - t
             st = r.stats
             row = {"schedule": name, "repeat": it, "total": r.total, "wall_s": wall, "kernel_ms": st["kernel_ms"],
                    "schedule_ms": st["schedule_ms"], "makespan_ms": st["makespan_ms"],
-                   "tail_idle_frac": st["tail_idle_frac"], "expand_ms": st["expand_ms"]}
+                   "tail_idle_frac": st["tail_idle_frac"], "expand_ms": st["expand_ms"], "tasks": st["tasks"]}
             out["runs"].append(row)
             print(json.dumps(row), flush=True)
     if args.json:

@@ -423,6 +423,10 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                             if (DIH) {
                                 load_class(p, t, dih);
                                 done *= dih.w;
+                                // The task's own row follows the class rules too
+                                // (the step applies them to children only).
+                                const uint32_t pc = (uint32_t)__popc(cols);
+                                if (avail && pc > dih.side_popc) avail &= pc == 31u ? dih.last_mask : p.noside;
                             }
                             const uint32_t own = p.owner_of ? __ldg(p.owner_of + t) : (uint32_t)t;
                             if (PER_OWNER) {
