@@ -75,3 +75,11 @@ def test_rejects_class_index_out_of_range(gpu):
     bad[0] = len(classes)
     with pytest.raises(gpu.NQError):
         gpu.count_dihedral_tasks(12, 4, c, l, r, bad)
+
+
+def test_cli_dihedral(gpu):
+    import re
+    import subprocess
+    exe = os.path.join(os.path.dirname(os.path.dirname(__file__)), "n_queens_b200", "n_queens")
+    out = subprocess.run([exe, "16", "5", "--dihedral"], capture_output=True, text=True, timeout=120).stdout
+    assert re.search(r"cuda 16 queens result 14772512, calc time", out), out
