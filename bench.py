@@ -24,6 +24,10 @@ Reported (one JSON line from rank 0):
              numSMs x 4 schedulers x clock;
   cpu_baseline  the reference's own CPU recursion (oracle/_ref, all host
              threads) on a seeded sample of the same tasks.
+  dihedral   the same whole-board count through the 8-fold decomposition
+             (nq_count_dihedral, prefix depth k+1), timed through the public
+             API after the measured arms; it visits fewer DFS nodes, so it is
+             reported as time per count, not in `value`.
 
 `--impl reference` times only that reference CPU path (rank 0; other ranks
 exit 0).  Under torchrun each rank counts the same board on its own GPU
@@ -77,6 +81,7 @@ def parse_args():
     ap.add_argument("--schedule", choices=["learned", "plain"], default="learned",
                     help="queue order of the headline arm; the other order is timed beside it")
     ap.add_argument("--no-compare", action="store_true", help="skip timing the other queue order")
+    ap.add_argument("--no-dihedral", action="store_true", help="skip timing the dihedral decomposition")
     return ap.parse_args()
 
 
@@ -430,6 +435,32 @@ def run_ours(args, world, rank, local):
                    else "n_queens_b200.count (nq_count)",
         }
 
+    # The same count through the 8-fold decomposition (fewer nodes, same
+    # total): wall and kernel time per count through nq_count_dihedral.
+    dihedral = None
+    if not args.no_dihedral and N >= 6:
+        kd = min(k + 1, N - 2)
+        dcfg = nq.Config()
+        dcfg.device = local
+        r = nq.count_dihedral(N, kd, config=dcfg)  # sizes the buffers
+        if r.total != want:
+            raise SystemExit(f"dihedral: count {r.total}, want {want}")
+        barrier(world)
+        walls, kms = [], []
+        for i in range(args.steps):
+            t0 = time.perf_counter()
+            r = nq.count_dihedral(N, kd, config=dcfg)
+            walls.append(time.perf_counter() - t0)
+            if r.total != want:
+                raise SystemExit(f"dihedral step {i}: count {r.total}, want {want}")
+            kms.append(r.stats["kernel_ms"])
+        barrier(world)
+        d_max = max_over_ranks(world, sum(walls))
+        dihedral = {"rows": kd, "tasks": int(r.stats["tasks"]), "count_ok": True,
+                    "wall_ms_per_step": 1000 * d_max / args.steps, "kernel_ms_per_step": statistics.mean(kms),
+                    "speedup_vs_headline_step": (1000 * t_max / args.steps) / (1000 * d_max / args.steps),
+                    "api": "n_queens_b200.count_dihedral (nq_count_dihedral)"}
+
     peak_clock = None
     try:
         peak_clock = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("sm_max_mhz")
@@ -473,7 +504,7 @@ def run_ours(args, world, rank, local):
                        "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"replicas x{world}",
                        "stack_levels": levels},
             "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-            "compare": compare, "model_build": build, "schedule_ms_per_step": sched_ms,
+            "compare": compare, "dihedral": dihedral, "model_build": build, "schedule_ms_per_step": sched_ms,
             # our kernels per timed step: learned = predict + bin + DFS (the radix sort between
             # them is CUB's), plain = DFS
             "gpu_launches": sum(args.steps * (3 if a == "learned" else 1) for a in arms),
