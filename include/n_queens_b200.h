@@ -324,11 +324,14 @@ typedef struct {
 int nq_dihedral_expand(int N, int rows, uint32_t *cols, uint32_t *ld, uint32_t *rd, uint8_t *cls, int64_t cap,
                        int64_t *n_tasks, nq_dihedral_class *classes, int cap_classes, int *n_classes);
 /* Whole-board total through the dihedral decomposition (the same total as
- * nq_count / cuda_n_queens).  stats->tasks counts the dihedral tasks. */
+ * nq_count / cuda_n_queens).  stats->tasks counts the dihedral tasks.  cfg's
+ * launch fields apply; device_expand does not (the tasks are built on the
+ * host). */
 int nq_count_dihedral(int N, int rows, const nq_config *cfg, uint64_t *total, nq_stats *stats);
 /* Weighted counts of a caller's dihedral tasks (host arrays, the classes of
  * (N, rows)): per_task[i] (optional) receives task i's weighted count, *sum
- * their sum. */
+ * their sum.  The tasks are meant to come from nq_dihedral_expand (any subset
+ * or order): on-board masks, ld/rd as the expander packs them. */
 int nq_count_dihedral_tasks(int N, int rows, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd,
                             const uint8_t *cls, int64_t n, uint64_t *per_task, uint64_t *sum, const nq_config *cfg,
                             nq_stats *stats);
