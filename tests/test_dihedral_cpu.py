@@ -62,3 +62,72 @@ def test_dihedral_rejects_bad_arguments(N, k):
         nq.dihedral_expand(N, k)
     with pytest.raises(nq.NQError):
         nq.count_dihedral(N, k)
+
+
+def _solutions(N):
+    out, q = [], []
+
+    def rec(row, cols, d1, d2):
+        if row == N:
+            out.append(tuple(q))
+            return
+        for c in range(N):
+            if c in cols or (row + c) in d1 or (row - c) in d2:
+                continue
+            q.append(c)
+            rec(row + 1, cols | {c}, d1 | {row + c}, d2 | {row - c})
+            q.pop()
+
+    rec(0, frozenset(), frozenset(), frozenset())
+    return out
+
+
+def _images(q):
+    N = len(q)
+    cells = [(r, c) for r, c in enumerate(q)]
+    maps = [lambda r, c: (r, c), lambda r, c: (c, N - 1 - r), lambda r, c: (N - 1 - r, N - 1 - c),
+            lambda r, c: (N - 1 - c, r), lambda r, c: (r, N - 1 - c), lambda r, c: (N - 1 - r, c),
+            lambda r, c: (c, r), lambda r, c: (N - 1 - c, N - 1 - r)]
+    imgs = set()
+    for f in maps:
+        b = [0] * N
+        for r, c in cells:
+            rr, cc = f(r, c)
+            b[rr] = cc
+        imgs.add(tuple(b))
+    return imgs
+
+
+@pytest.mark.parametrize("N", range(6, 12))
+def test_every_orbit_gets_its_size(N):
+    # Each solution is counted by the tasks whose prefix it extends, under their
+    # classes' rules and weights; over every orbit of the eight symmetries of the
+    # square the weights must add up to the orbit's size.
+    sols = _solutions(N)
+    for k in range(2, min(6, N - 1)):
+        c, l, r, cls, classes = oracle.dihedral_expand(N, k)
+        by_prefix = {}
+        for i in range(c.size):
+            by_prefix.setdefault((int(c[i]), int(l[i]), int(r[i])), []).append(classes[int(cls[i])])
+        weight = {}
+        for q in sols:
+            cc = ll = rr = 0
+            for i in range(k):
+                p = 1 << q[i]
+                cc, ll, rr = cc | p, ((ll | p) << 1) & 0xFFFFFFFF, (rr | p) >> 1
+            w = 0
+            for side_row, last_mask, tie_bit, wt, wt_tie in by_prefix.get((cc, ll, rr), []):
+                if any(i > side_row and q[i] in (0, N - 1) for i in range(k, N)):
+                    continue
+                last = 1 << q[N - 1]
+                if not last & last_mask:
+                    continue
+                w += wt_tie if last == tie_bit else wt
+            weight[q] = w
+        seen = set()
+        for q in sols:
+            if q in seen:
+                continue
+            orbit = _images(q)
+            seen |= orbit
+            assert sum(weight[s] for s in orbit) == len(orbit), (N, k, q)
