@@ -329,6 +329,12 @@ int nq_dihedral_expand(int N, int rows, uint32_t *cols, uint32_t *ld, uint32_t *
  * launch fields apply; device_expand does not (the tasks are built on the
  * host). */
 int nq_count_dihedral(int N, int rows, const nq_config *cfg, uint64_t *total, nq_stats *stats);
+/* nq_count_resumable through the dihedral decomposition: the same slices,
+ * checkpoint file and guarantees (every saved level keeps its class); a
+ * checkpoint of the other decomposition is rejected with NQ_ERR_ARG.
+ * CLI: n_queens N rows --dihedral --checkpoint PATH [--slice-ms MS]. */
+int nq_count_dihedral_resumable(int N, int rows, const nq_config *cfg, const char *checkpoint_path, uint64_t *total,
+                                int *done, nq_stats *stats);
 /* Weighted counts of a caller's dihedral tasks (host arrays, the classes of
  * (N, rows)): per_task[i] (optional) receives task i's weighted count, *sum
  * their sum.  The tasks are meant to come from nq_dihedral_expand (any subset

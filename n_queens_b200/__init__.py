@@ -178,6 +178,9 @@ def _load() -> ctypes.CDLL:
                                      ctypes.POINTER(DihedralClass), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.nq_count_dihedral.restype = ctypes.c_int
     L.nq_count_dihedral.argtypes = [ctypes.c_int, ctypes.c_int, _cfgp, _u64p, _stp]
+    L.nq_count_dihedral_resumable.restype = ctypes.c_int
+    L.nq_count_dihedral_resumable.argtypes = [ctypes.c_int, ctypes.c_int, _cfgp, ctypes.c_char_p, _u64p,
+                                              ctypes.POINTER(ctypes.c_int), _stp]
     L.nq_count_dihedral_tasks.restype = ctypes.c_int
     L.nq_count_dihedral_tasks.argtypes = [ctypes.c_int, ctypes.c_int, _u32p, _u32p, _u32p, _u8p, ctypes.c_int64,
                                           _u64p, _u64p, _cfgp, _stp]
@@ -194,7 +197,8 @@ EXPORTS = ("nq_abi_version", "nq_status_string", "nq_last_error", "nq_device_cou
            "nq_batch_create", "nq_batch_run", "nq_batch_destroy", "nq_batch_autotune",
            "nq_mlp_num_params", "nq_mlp_create", "nq_mlp_destroy", "nq_mlp_get_params", "nq_mlp_set_params",
            "nq_mlp_predict", "nq_mlp_predict_tensor", "nq_mlp_grad", "nq_mlp_train", "nq_schedule_device", "nq_count_learned",
-           "nq_dihedral_expand", "nq_count_dihedral", "nq_count_dihedral_tasks")
+           "nq_dihedral_expand", "nq_count_dihedral", "nq_count_dihedral_tasks",
+           "nq_count_dihedral_resumable")
 
 
 def status_string(status: int) -> str:
@@ -313,8 +317,9 @@ def count_dihedral_tasks(N: int, rows: int, cols, ld, rd, cls, per_task: bool = 
     return {"sum": int(s.value), "per_task": pt, "stats": st.as_dict()}
 
 
-def count_resumable(N: int, rows: int, checkpoint: str, slice_ms: int = 0, config=None):
-    """One slice of a resumable whole-board count (``nq_count_resumable``).
+def count_resumable(N: int, rows: int, checkpoint: str, slice_ms: int = 0, config=None, dihedral: bool = False):
+    """One slice of a resumable whole-board count (``nq_count_resumable``, or
+    ``nq_count_dihedral_resumable`` with ``dihedral=True``).
 
     Returns (done, total, stats); total is valid once done.  Call again with
     the same checkpoint path until done.
@@ -329,9 +334,10 @@ def count_resumable(N: int, rows: int, checkpoint: str, slice_ms: int = 0, confi
     tot = ctypes.c_uint64(0)
     done = ctypes.c_int(0)
     st = Stats()
-    rc = lib.nq_count_resumable(N, rows, ctypes.byref(c), os.fsencode(checkpoint), ctypes.byref(tot),
-                                ctypes.byref(done), ctypes.byref(st))
-    _check(rc, "nq_count_resumable")
+    fn = lib.nq_count_dihedral_resumable if dihedral else lib.nq_count_resumable
+    rc = fn(N, rows, ctypes.byref(c), os.fsencode(checkpoint), ctypes.byref(tot), ctypes.byref(done),
+            ctypes.byref(st))
+    _check(rc, "nq_count_dihedral_resumable" if dihedral else "nq_count_resumable")
     return bool(done.value), int(tot.value), st.as_dict()
 
 

@@ -173,6 +173,8 @@ int ensure_ready(Ctx &c, int dev) {
                                              c.smem_optin - static_smem));
     NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, 1, 8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  c.smem_optin - static_smem));
+    NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, 1, 8, true, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, c.smem_optin - static_smem));
     for (int po = 0; po < 2; ++po)
         NQ_CUDA(cudaFuncSetAttribute(pick_kernel(po, false, -1, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      c.smem_optin - static_smem));
@@ -447,36 +449,70 @@ int count_resident(Ctx &c, int N, const uint32_t *d_cols, const uint32_t *d_ld, 
 
 
 
+// Uploads the class table of (N, rows) behind `used` bytes of c.tasks and
+// fills the launch's class arguments.  The caller has grown c.tasks.
+int dih_upload_classes(Ctx &c, int N, int rows, size_t used, DihArgs &a) {
+    std::vector<DihClass> tab;
+    if (!dihedral_classes(N, rows, tab) || tab.size() > (size_t)kMaxDihClasses) return NQ_ERR_ARG;
+    uint4 h[kMaxDihClasses];  // synchronous copy below: the array may go out of scope after it
+    for (size_t i = 0; i < tab.size(); ++i) {
+        const DihClass &t = tab[i];
+        // popc of a child's column mask (off-board bits set) is 32 - N + its
+        // row; rows beyond side_row are popc values beyond this threshold.
+        const int thr = 32 - N + t.side_row;
+        h[i] = make_uint4((uint32_t)std::min(thr, 64), t.last_mask, t.tie_bit, t.w | (t.w_tie << 16));
+    }
+    const size_t off = (used + 255) & ~(size_t)255;
+    uint4 *d = (uint4 *)((char *)c.tasks.p + off);
+    NQ_CUDA(cudaMemcpy(d, h, tab.size() * sizeof(uint4), cudaMemcpyHostToDevice));
+    a.cls_tab = d;
+    a.noside = ~(1u | (1u << (N - 1)));
+    return NQ_OK;
+}
+
+size_t dih_bytes(int64_t n) {
+    return (((size_t)std::max<int64_t>(n, 1) * 13 + 255) & ~(size_t)255) + kMaxDihClasses * sizeof(uint4);
+}
+
 // Checkpoint of a resumable whole-board count (little-endian file):
-//   "NQB200CK" | u32 version=1 | i32 N | i32 rows | i32 0 | i64 ntasks |
+//   "NQB200CK" | u32 version=1 | i32 N | i32 rows | i32 mode | i64 ntasks |
 //   i64 cursor | u64 partial (plain sum so far) | u64 slices | i64 n_cont |
-//   n_cont x 16-byte continuation entries (cols|~last, ld, rd, untried)
+//   n_cont x 16-byte continuation entries (cols|~last, ld, rd, untried) |
+//   mode 1 only: n_cont class-index bytes
+// mode 0 is the reference's decomposition (the partial sum is doubled at the
+// end), mode 1 the dihedral one (the partial sum is weighted already).
 struct Checkpoint {
     int N = 0, rows = 0;
+    int mode = 0;  // 0: the reference's decomposition, 1: the dihedral one
     int64_t ntasks = 0, cursor = 0;
     uint64_t partial = 0, slices = 0;
     std::vector<uint4> cont;
+    std::vector<uint8_t> cls;  // mode 1: class index of each continuation entry
 };
 
 const char kCkMagic[8] = {'N', 'Q', 'B', '2', '0', '0', 'C', 'K'};
 
-int read_checkpoint(const char *path, int N, int rows, Checkpoint &ck, bool &have) {
+int read_checkpoint(const char *path, int N, int rows, int mode, Checkpoint &ck, bool &have) {
     have = false;
     FILE *f = std::fopen(path, "rb");
     if (!f) return NQ_OK;  // no checkpoint yet: start from the beginning
     char magic[8];
     uint32_t version = 0;
-    int32_t hN = 0, hrows = 0, pad = 0;
+    int32_t hN = 0, hrows = 0, hmode = 0;
     int64_t n_cont = -1;
     bool ok = std::fread(magic, 1, 8, f) == 8 && memcmp(magic, kCkMagic, 8) == 0 &&
               std::fread(&version, 4, 1, f) == 1 && version == 1 && std::fread(&hN, 4, 1, f) == 1 &&
-              std::fread(&hrows, 4, 1, f) == 1 && std::fread(&pad, 4, 1, f) == 1 &&
+              std::fread(&hrows, 4, 1, f) == 1 && std::fread(&hmode, 4, 1, f) == 1 && (hmode == 0 || hmode == 1) &&
               std::fread(&ck.ntasks, 8, 1, f) == 1 && std::fread(&ck.cursor, 8, 1, f) == 1 &&
               std::fread(&ck.partial, 8, 1, f) == 1 && std::fread(&ck.slices, 8, 1, f) == 1 &&
               std::fread(&n_cont, 8, 1, f) == 1 && n_cont >= 0 && n_cont < (int64_t)1 << 32;
     if (ok) {
         ck.cont.resize((size_t)n_cont);
         ok = n_cont == 0 || std::fread(ck.cont.data(), 16, (size_t)n_cont, f) == (size_t)n_cont;
+        if (ok && hmode == 1) {
+            ck.cls.resize((size_t)n_cont);
+            ok = n_cont == 0 || std::fread(ck.cls.data(), 1, (size_t)n_cont, f) == (size_t)n_cont;
+        }
         char extra;
         ok = ok && std::fread(&extra, 1, 1, f) == 0;  // nothing after the entries
     }
@@ -489,8 +525,13 @@ int read_checkpoint(const char *path, int N, int rows, Checkpoint &ck, bool &hav
         g_last_error = "checkpoint is for N=" + std::to_string(hN) + " rows=" + std::to_string(hrows);
         return NQ_ERR_ARG;
     }
+    if (hmode != mode) {
+        g_last_error = hmode ? "checkpoint is of a dihedral count" : "checkpoint is of a plain (mirror) count";
+        return NQ_ERR_ARG;
+    }
     ck.N = hN;
     ck.rows = hrows;
+    ck.mode = hmode;
     have = true;
     return NQ_OK;
 }
@@ -503,14 +544,15 @@ int write_checkpoint(const char *path, const Checkpoint &ck) {
         return NQ_ERR_ARG;
     }
     const uint32_t version = 1;
-    const int32_t hN = ck.N, hrows = ck.rows, pad = 0;
+    const int32_t hN = ck.N, hrows = ck.rows, hmode = ck.mode;
     const int64_t n_cont = (int64_t)ck.cont.size();
     bool ok = std::fwrite(kCkMagic, 1, 8, f) == 8 && std::fwrite(&version, 4, 1, f) == 1 &&
-              std::fwrite(&hN, 4, 1, f) == 1 && std::fwrite(&hrows, 4, 1, f) == 1 && std::fwrite(&pad, 4, 1, f) == 1 &&
-              std::fwrite(&ck.ntasks, 8, 1, f) == 1 && std::fwrite(&ck.cursor, 8, 1, f) == 1 &&
-              std::fwrite(&ck.partial, 8, 1, f) == 1 && std::fwrite(&ck.slices, 8, 1, f) == 1 &&
-              std::fwrite(&n_cont, 8, 1, f) == 1 &&
-              (n_cont == 0 || std::fwrite(ck.cont.data(), 16, (size_t)n_cont, f) == (size_t)n_cont);
+              std::fwrite(&hN, 4, 1, f) == 1 && std::fwrite(&hrows, 4, 1, f) == 1 &&
+              std::fwrite(&hmode, 4, 1, f) == 1 && std::fwrite(&ck.ntasks, 8, 1, f) == 1 &&
+              std::fwrite(&ck.cursor, 8, 1, f) == 1 && std::fwrite(&ck.partial, 8, 1, f) == 1 &&
+              std::fwrite(&ck.slices, 8, 1, f) == 1 && std::fwrite(&n_cont, 8, 1, f) == 1 &&
+              (n_cont == 0 || std::fwrite(ck.cont.data(), 16, (size_t)n_cont, f) == (size_t)n_cont) &&
+              (ck.mode == 0 || n_cont == 0 || std::fwrite(ck.cls.data(), 1, (size_t)n_cont, f) == (size_t)n_cont);
     ok = (std::fflush(f) == 0) && ok;
     std::fclose(f);
     if (!ok || std::rename(tmp.c_str(), path) != 0) {
@@ -732,6 +774,175 @@ void set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
 
 }  // namespace nqb
 
+namespace nqb {
+namespace {
+
+// One slice of a resumable whole-board count, in the reference's
+// decomposition (dih false) or the dihedral one (dih true).
+int count_resumable_impl(int N, int rows, const nq_config *cfg, const char *checkpoint_path, bool dih,
+                         uint64_t *total, int *done, nq_stats *stats) {
+    const double t0 = now_ms();
+    if (stats) memset(stats, 0, sizeof(*stats));
+    *done = 0;
+    *total = 0;
+    Checkpoint ck;
+    bool have = false;
+    int rc = read_checkpoint(checkpoint_path, N, rows, dih ? 1 : 0, ck, have);
+    if (rc) return rc;
+    Ctx *cp = nullptr;
+    rc = lock_device(device_of(cfg), cp);
+    if (rc) return rc;
+    Ctx &c = *cp;
+    std::lock_guard<std::mutex> lock(c.mu);
+    rc = ensure_ready(c, device_of(cfg));
+    if (rc) return rc;
+    const double te = now_ms();
+    const int64_t n = dih ? dihedral_expand(N, rows, nullptr, nullptr, nullptr, nullptr, 0)
+                          : expand_prefixes(N, rows, nullptr, nullptr, nullptr, 0, 0);
+    if (n < 0 || n > 0xffffffffll) return NQ_ERR_ARG;
+    if (have && (ck.ntasks != n || ck.cursor < 0 || ck.cursor > n)) {
+        g_last_error = "checkpoint does not match this board's task list";
+        return NQ_ERR_ARG;
+    }
+    const size_t ncont = have ? ck.cont.size() : 0;
+    const size_t per_task = dih ? 13 : 12;  // cols | ld | rd (u32) [| class (u8)]
+    rc = c.h_tasks.grow((size_t)std::max<int64_t>(n, 1) * per_task);
+    if (rc) return rc;
+    uint32_t *h = (uint32_t *)c.h_tasks.p;
+    if (dih)
+        dihedral_expand(N, rows, h, h + n, h + 2 * n, (uint8_t *)(h + 3 * n), n);
+    else
+        expand_prefixes(N, rows, h, h + n, h + 2 * n, n, 0);
+    if (stats) {
+        stats->expand_ms = now_ms() - te;
+        stats->tasks = n;
+    }
+    // tasks [+ classes + class table], then the continuation entries to resume
+    // [and their class indices]
+    const size_t task_bytes = dih ? dih_bytes(n) : (((size_t)std::max<int64_t>(n, 1) * 12 + 255) & ~(size_t)255);
+    rc = c.tasks.grow(task_bytes + ncont * 17 + 512);
+    if (rc) return rc;
+    uint32_t *d = (uint32_t *)c.tasks.p;
+    uint4 *d_cont_in = (uint4 *)((char *)c.tasks.p + task_bytes);
+    uint8_t *d_cont_cls = (uint8_t *)(d_cont_in + ncont);
+    DihArgs a;
+    if (dih) {
+        a.task_cls = (const uint8_t *)(d + 3 * n);
+        rc = dih_upload_classes(c, N, rows, (size_t)n * 13, a);
+        if (rc) return rc;
+        for (size_t i = 0; i < ncont; ++i)
+            if (ck.cls[i] >= kMaxDihClasses) {
+                g_last_error = "checkpoint holds a class index out of range";
+                return NQ_ERR_ARG;
+            }
+    }
+    NQ_CUDA(cudaEventRecord(c.ev[0], c.stream));
+    if (n) NQ_CUDA(cudaMemcpyAsync(d, h, (size_t)n * per_task, cudaMemcpyHostToDevice, c.stream));
+    if (ncont) {
+        NQ_CUDA(cudaMemcpyAsync(d_cont_in, ck.cont.data(), ncont * 16, cudaMemcpyHostToDevice, c.stream));
+        if (dih) NQ_CUDA(cudaMemcpyAsync(d_cont_cls, ck.cls.data(), ncont, cudaMemcpyHostToDevice, c.stream));
+    }
+    KernelFn fn = dih ? dfs_kernel<false, false, 1, 8, true, true> : dfs_kernel<false, false, 1, 8, true>;
+    Launch L;
+    rc = plan_launch(c, cfg, N - 1 - rows, false, false, L, dih);
+    if (rc) return rc;
+    {
+        // the resumable instantiation may fit fewer CTAs per SM
+        int per_sm = 0;
+        NQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, L.threads, L.smem));
+        if (per_sm <= 0) return NQ_ERR_ARG;
+        L.grid = std::min(L.grid, c.sms * std::min(per_sm, kMaxBlocksPerSm));
+    }
+    fill_stats_launch(stats, L);
+    // room for every lane's unfinished levels: the current one + one per slot
+    const size_t cap = (size_t)L.grid * L.threads * (L.levels + 1);
+    rc = c.aux.grow(cap * (dih ? 17 : 16));
+    if (rc) return rc;
+    DfsParams p = base_params(c, N, n, cfg);
+    p.cols = d;
+    p.ld = d + n;
+    p.rd = d + 2 * n;
+    p.cont_in = d_cont_in;
+    p.n_cont_in = (long long)ncont;
+    p.task_base = have ? ck.cursor : 0;
+    p.cont_out = (uint4 *)c.aux.p;
+    p.cont_cap = (long long)cap;
+    if (dih) {
+        p.task_cls = a.task_cls;
+        p.cls_tab = a.cls_tab;
+        p.noside = a.noside;
+        p.cont_in_cls = d_cont_cls;
+        p.cont_out_cls = (uint8_t *)((uint4 *)c.aux.p + cap);
+    }
+    p.levels = L.levels;
+    p.inner = L.inner;
+    p.steal = L.steal;
+    p.layout = L.layout;
+    NQ_CUDA(cudaEventRecord(c.ev[1], c.stream));
+    NQ_CUDA(cudaMemsetAsync(p.ctl, 0, kCtlWords * sizeof(unsigned long long), c.stream));
+    fn<<<L.grid, L.threads, L.smem, c.stream>>>(p);
+    NQ_CUDA(cudaGetLastError());
+    NQ_CUDA(cudaEventRecord(c.ev[2], c.stream));
+    unsigned long long words[kWordBlocks];
+    NQ_CUDA(cudaMemcpyAsync(words, c.d_ctl, sizeof(words), cudaMemcpyDeviceToHost, c.stream));
+    NQ_CUDA(cudaStreamSynchronize(c.stream));
+    if (stats) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]);
+        stats->h2d_ms = ms;
+        cudaEventElapsedTime(&ms, c.ev[1], c.ev[2]);
+        stats->kernel_ms = ms;
+    }
+    const unsigned long long bits = words[kWordStatus];
+    if (bits & kStatContOverflow) {
+        g_last_error = "continuation buffer overflow";
+        return NQ_ERR_CUDA;
+    }
+    if (bits & kStatDepth) return status_from_bits(bits);
+    const uint64_t partial = (have ? ck.partial : 0) + words[kWordSum];
+    if (bits & kStatTimeout) {
+        // Positions taken from the queue were either finished or saved.
+        const long long qlen = (long long)ncont + n - p.task_base;
+        const long long taken = std::min<long long>((long long)words[kCtlHead], qlen);
+        Checkpoint out;
+        out.N = N;
+        out.rows = rows;
+        out.mode = dih ? 1 : 0;
+        out.ntasks = n;
+        out.cursor = p.task_base + std::max<long long>(0, taken - (long long)ncont);
+        out.partial = partial;
+        out.slices = (have ? ck.slices : 0) + 1;
+        // Saved levels of an earlier slice that no lane picked up this time
+        // carry over unchanged, then come the levels this slice saved.
+        const size_t untaken = (size_t)std::max<long long>(0, (long long)ncont - taken);
+        const size_t fresh = (size_t)words[kCtlCont];
+        out.cont.resize(untaken + fresh);
+        for (size_t i = 0; i < untaken; ++i) out.cont[i] = ck.cont[ncont - untaken + i];
+        if (fresh)
+            NQ_CUDA(cudaMemcpy(out.cont.data() + untaken, c.aux.p, fresh * 16, cudaMemcpyDeviceToHost));
+        if (dih) {
+            out.cls.resize(untaken + fresh);
+            for (size_t i = 0; i < untaken; ++i) out.cls[i] = ck.cls[ncont - untaken + i];
+            if (fresh)
+                NQ_CUDA(cudaMemcpy(out.cls.data() + untaken, p.cont_out_cls, fresh, cudaMemcpyDeviceToHost));
+        }
+        rc = write_checkpoint(checkpoint_path, out);
+        if (rc) return rc;
+        if (stats) stats->total_ms = now_ms() - t0;
+        return NQ_OK;
+    }
+    // The reference doubles the half-board sum (src/n_queens_cuda.cu:181-183);
+    // dihedral weights already carry every symmetry factor.
+    *total = dih ? partial : 2 * partial;
+    *done = 1;
+    if (have) std::remove(checkpoint_path);
+    if (stats) stats->total_ms = now_ms() - t0;
+    return NQ_OK;
+}
+
+}  // namespace
+}  // namespace nqb
+
 using namespace nqb;
 
 extern "C" {
@@ -885,128 +1096,16 @@ int nq_count(int N, int rows, const nq_config *cfg, uint64_t *total, uint64_t *n
 
 int nq_count_resumable(int N, int rows, const nq_config *cfg, const char *checkpoint_path, uint64_t *total,
                        int *done, nq_stats *stats) {
-    const double t0 = now_ms();
     if (stats) memset(stats, 0, sizeof(*stats));
     if (N < 2 || N > NQ_MAX_N || rows < 1 || rows > N - 2 || !total || !done || !checkpoint_path) return NQ_ERR_ARG;
-    *done = 0;
-    *total = 0;
-    Checkpoint ck;
-    bool have = false;
-    int rc = read_checkpoint(checkpoint_path, N, rows, ck, have);
-    if (rc) return rc;
-    Ctx *cp = nullptr;
-    rc = lock_device(device_of(cfg), cp);
-    if (rc) return rc;
-    Ctx &c = *cp;
-    std::lock_guard<std::mutex> lock(c.mu);
-    rc = ensure_ready(c, device_of(cfg));
-    if (rc) return rc;
-    const double te = now_ms();
-    const int64_t n = expand_prefixes(N, rows, nullptr, nullptr, nullptr, 0, 0);
-    if (n < 0) return NQ_ERR_ARG;
-    if (have && (ck.ntasks != n || ck.cursor < 0 || ck.cursor > n)) {
-        g_last_error = "checkpoint does not match this board's task list";
-        return NQ_ERR_ARG;
-    }
-    const size_t ncont = have ? ck.cont.size() : 0;
-    rc = c.h_tasks.grow((size_t)std::max<int64_t>(n, 1) * 12);
-    if (rc) return rc;
-    uint32_t *h = (uint32_t *)c.h_tasks.p;
-    expand_prefixes(N, rows, h, h + n, h + 2 * n, n, 0);
-    if (stats) {
-        stats->expand_ms = now_ms() - te;
-        stats->tasks = n;
-    }
-    // tasks, then the continuation entries to resume
-    const size_t task_bytes = ((size_t)std::max<int64_t>(n, 1) * 12 + 255) & ~(size_t)255;
-    rc = c.tasks.grow(task_bytes + ncont * 16 + 256);
-    if (rc) return rc;
-    uint32_t *d = (uint32_t *)c.tasks.p;
-    uint4 *d_cont_in = (uint4 *)((char *)c.tasks.p + task_bytes);
-    NQ_CUDA(cudaEventRecord(c.ev[0], c.stream));
-    if (n) NQ_CUDA(cudaMemcpyAsync(d, h, (size_t)n * 12, cudaMemcpyHostToDevice, c.stream));
-    if (ncont)
-        NQ_CUDA(cudaMemcpyAsync(d_cont_in, ck.cont.data(), ncont * 16, cudaMemcpyHostToDevice, c.stream));
-    Launch L;
-    rc = plan_launch(c, cfg, N - 1 - rows, false, false, L);
-    if (rc) return rc;
-    {
-        // the resumable instantiation may fit fewer CTAs per SM
-        int per_sm = 0;
-        NQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dfs_kernel<false, false, 1, 8, true>,
-                                                              L.threads, L.smem));
-        if (per_sm <= 0) return NQ_ERR_ARG;
-        L.grid = std::min(L.grid, c.sms * std::min(per_sm, kMaxBlocksPerSm));
-    }
-    fill_stats_launch(stats, L);
-    // room for every lane's unfinished levels: the current one + one per slot
-    const size_t cap = (size_t)L.grid * L.threads * (L.levels + 1);
-    rc = c.aux.grow(cap * 16);
-    if (rc) return rc;
-    DfsParams p = base_params(c, N, n, cfg);
-    p.cols = d;
-    p.ld = d + n;
-    p.rd = d + 2 * n;
-    p.cont_in = d_cont_in;
-    p.n_cont_in = (long long)ncont;
-    p.task_base = have ? ck.cursor : 0;
-    p.cont_out = (uint4 *)c.aux.p;
-    p.cont_cap = (long long)cap;
-    p.levels = L.levels;
-    p.inner = L.inner;
-    p.steal = L.steal;
-    p.layout = L.layout;
-    NQ_CUDA(cudaEventRecord(c.ev[1], c.stream));
-    NQ_CUDA(cudaMemsetAsync(p.ctl, 0, kCtlWords * sizeof(unsigned long long), c.stream));
-    dfs_kernel<false, false, 1, 8, true><<<L.grid, L.threads, L.smem, c.stream>>>(p);
-    NQ_CUDA(cudaGetLastError());
-    NQ_CUDA(cudaEventRecord(c.ev[2], c.stream));
-    unsigned long long words[kWordBlocks];
-    NQ_CUDA(cudaMemcpyAsync(words, c.d_ctl, sizeof(words), cudaMemcpyDeviceToHost, c.stream));
-    NQ_CUDA(cudaStreamSynchronize(c.stream));
-    if (stats) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, c.ev[0], c.ev[1]);
-        stats->h2d_ms = ms;
-        cudaEventElapsedTime(&ms, c.ev[1], c.ev[2]);
-        stats->kernel_ms = ms;
-    }
-    const unsigned long long bits = words[kWordStatus];
-    if (bits & kStatContOverflow) {
-        g_last_error = "continuation buffer overflow";
-        return NQ_ERR_CUDA;
-    }
-    if (bits & kStatDepth) return status_from_bits(bits);
-    const uint64_t partial = (have ? ck.partial : 0) + words[kWordSum];
-    if (bits & kStatTimeout) {
-        // Positions taken from the queue were either finished or saved.
-        const long long qlen = (long long)ncont + n - p.task_base;
-        const long long taken = std::min<long long>((long long)words[kCtlHead], qlen);
-        Checkpoint out;
-        out.N = N;
-        out.rows = rows;
-        out.ntasks = n;
-        out.cursor = p.task_base + std::max<long long>(0, taken - (long long)ncont);
-        out.partial = partial;
-        out.slices = (have ? ck.slices : 0) + 1;
-        // Saved levels of an earlier slice that no lane picked up this time
-        // carry over unchanged, then come the levels this slice saved.
-        const size_t untaken = (size_t)std::max<long long>(0, (long long)ncont - taken);
-        const size_t fresh = (size_t)words[kCtlCont];
-        out.cont.resize(untaken + fresh);
-        for (size_t i = 0; i < untaken; ++i) out.cont[i] = ck.cont[ncont - untaken + i];
-        if (fresh)
-            NQ_CUDA(cudaMemcpy(out.cont.data() + untaken, c.aux.p, fresh * 16, cudaMemcpyDeviceToHost));
-        rc = write_checkpoint(checkpoint_path, out);
-        if (rc) return rc;
-        if (stats) stats->total_ms = now_ms() - t0;
-        return NQ_OK;
-    }
-    *total = 2 * partial;
-    *done = 1;
-    if (have) std::remove(checkpoint_path);
-    if (stats) stats->total_ms = now_ms() - t0;
-    return NQ_OK;
+    return count_resumable_impl(N, rows, cfg, checkpoint_path, false, total, done, stats);
+}
+
+int nq_count_dihedral_resumable(int N, int rows, const nq_config *cfg, const char *checkpoint_path, uint64_t *total,
+                                int *done, nq_stats *stats) {
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (N < 4 || N > NQ_MAX_N || rows < 2 || rows > N - 2 || !total || !done || !checkpoint_path) return NQ_ERR_ARG;
+    return count_resumable_impl(N, rows, cfg, checkpoint_path, true, total, done, stats);
 }
 
 int nq_count_learned(int N, int rows, nq_mlp *m, const nq_config *cfg, uint64_t *total, nq_stats *stats) {
@@ -1274,35 +1373,6 @@ int nq_dihedral_expand(int N, int rows, uint32_t *cols, uint32_t *ld, uint32_t *
     if (n_tasks) *n_tasks = n;
     return NQ_OK;
 }
-
-namespace {
-
-// Uploads the class table of (N, rows) behind `used` bytes of c.tasks and
-// fills the launch's class arguments.  The caller has grown c.tasks.
-int dih_upload_classes(Ctx &c, int N, int rows, size_t used, DihArgs &a) {
-    std::vector<DihClass> tab;
-    if (!dihedral_classes(N, rows, tab) || tab.size() > (size_t)kMaxDihClasses) return NQ_ERR_ARG;
-    uint4 h[kMaxDihClasses];  // synchronous copy below: the array may go out of scope after it
-    for (size_t i = 0; i < tab.size(); ++i) {
-        const DihClass &t = tab[i];
-        // popc of a child's column mask (off-board bits set) is 32 - N + its
-        // row; rows beyond side_row are popc values beyond this threshold.
-        const int thr = 32 - N + t.side_row;
-        h[i] = make_uint4((uint32_t)std::min(thr, 64), t.last_mask, t.tie_bit, t.w | (t.w_tie << 16));
-    }
-    const size_t off = (used + 255) & ~(size_t)255;
-    uint4 *d = (uint4 *)((char *)c.tasks.p + off);
-    NQ_CUDA(cudaMemcpy(d, h, tab.size() * sizeof(uint4), cudaMemcpyHostToDevice));
-    a.cls_tab = d;
-    a.noside = ~(1u | (1u << (N - 1)));
-    return NQ_OK;
-}
-
-size_t dih_bytes(int64_t n) {
-    return (((size_t)std::max<int64_t>(n, 1) * 13 + 255) & ~(size_t)255) + kMaxDihClasses * sizeof(uint4);
-}
-
-}  // namespace
 
 int nq_count_dihedral(int N, int rows, const nq_config *cfg, uint64_t *total, nq_stats *stats) {
     const double t0 = now_ms();

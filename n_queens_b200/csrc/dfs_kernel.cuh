@@ -97,6 +97,10 @@ struct DfsParams {
     const uint8_t *task_cls;
     const uint4 *cls_tab;
     uint32_t noside;                 // ~(column 0 | column N-1)
+    // Resumable dihedral runs: the class index of each continuation entry
+    // (in) and of each saved level (out).
+    const uint8_t *cont_in_cls;
+    uint8_t *cont_out_cls;
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -236,9 +240,10 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "selp.b32 w, %16, %15, px;\n\t"                                                   \
     "@pe add.u32 %5, %5, w;\n\t"
 
-// Class registers of a lane in a DIH kernel.
+// Class registers of a lane in a DIH kernel (cls: the class index, kept for
+// the deadline dump of resumable runs).
 struct DihLane {
-    uint32_t side_popc = 64u, last_mask = ~0u, tie_bit = 0u, w = 0u, w_tie = 0u;
+    uint32_t side_popc = 64u, last_mask = ~0u, tie_bit = 0u, w = 0u, w_tie = 0u, cls = 0u;
 };
 
 struct StepConsts {
@@ -276,13 +281,18 @@ __device__ __forceinline__ void dfs_step_dih(uint32_t &cols, uint32_t &ld, uint3
                  : "memory");
 }
 
-__device__ __forceinline__ void load_class(const DfsParams &p, long long t, DihLane &d) {
-    const uint4 c = __ldg(p.cls_tab + __ldg(p.task_cls + t));
+__device__ __forceinline__ void load_class_index(const DfsParams &p, uint32_t idx, DihLane &d) {
+    const uint4 c = __ldg(p.cls_tab + idx);
+    d.cls = idx;
     d.side_popc = c.x;
     d.last_mask = c.y;
     d.tie_bit = c.z;
     d.w = c.w & 0xffffu;
     d.w_tie = c.w >> 16;
+}
+
+__device__ __forceinline__ void load_class(const DfsParams &p, long long t, DihLane &d) {
+    load_class_index(p, __ldg(p.task_cls + t), d);
 }
 
 // Loads task t into a lane.  Returns the completions credited immediately
@@ -410,6 +420,8 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                             ld = e.y;
                             rd = e.z;
                             avail = e.w;
+                            // a saved level already carries its class's rules in avail
+                            if (DIH) load_class_index(p, p.cont_in_cls[q], dih);
                             if (PER_OWNER && avail) owner = p.cont_in_owner ? p.cont_in_owner[q] : 0u;
                         }
                     } else if (q < (unsigned long long)qlen) {
@@ -468,6 +480,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                             src_dih.tie_bit = __shfl_sync(kFull, dih.tie_bit, src);
                             src_dih.w = __shfl_sync(kFull, dih.w, src);
                             src_dih.w_tie = __shfl_sync(kFull, dih.w_tie, src);
+                            if (RESUME) src_dih.cls = __shfl_sync(kFull, dih.cls, src);
                         }
                         if (donor >= 0) {
                             lds128(src_addr, cols, ld, rd, avail);
@@ -531,6 +544,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
             if (avail) {
                 p.cont_out[at] = make_uint4(cols, ld, rd, avail);
                 if (p.cont_out_owner) p.cont_out_owner[at] = owner;
+                if (DIH) p.cont_out_cls[at] = (uint8_t)dih.cls;
                 ++at;
             }
             for (uint32_t a = bot; a != sp; a += stride, ++at) {
@@ -538,6 +552,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                 lds128(a, x, y, z, w);
                 p.cont_out[at] = make_uint4(x, y, z, w);
                 if (p.cont_out_owner) p.cont_out_owner[at] = owner;
+                if (DIH) p.cont_out_cls[at] = (uint8_t)dih.cls;
             }
         }
     }

@@ -23,7 +23,8 @@ int main(int argc, char *argv[]) {
     // slices of MS milliseconds and saves its state to PATH after each one, so
     // an interrupted run continues where it stopped when started again.
     // --dihedral (not in the reference) counts through the 8-fold
-    // decomposition (nq_count_dihedral): same total, fewer DFS nodes.
+    // decomposition (nq_count_dihedral, or nq_count_dihedral_resumable with
+    // --checkpoint): same total, fewer DFS nodes.
     const char *ckpt = nullptr;
     unsigned slice_ms = 600000;
     bool dihedral = false;
@@ -35,10 +36,6 @@ int main(int argc, char *argv[]) {
             else if (!strcmp(argv[a], "--slice-ms")) slice_ms = (unsigned)strtoul(argv[a + 1], nullptr, 10);
             ++a;
         }
-    }
-    if (dihedral && ckpt) {
-        printf("--dihedral and --checkpoint cannot be combined\n");
-        return -1;
     }
     int N = atoi(argv[1]);
     if (N < 2 || N > 28) {
@@ -74,7 +71,10 @@ int main(int argc, char *argv[]) {
         for (int slice = 1;; ++slice) {
             uint64_t total = 0;
             int done = 0;
-            const int rc = nq_count_resumable(N, rows, &cfg, ckpt, &total, &done, nullptr);
+            const int rc = dihedral ? (N < 4 ? NQ_OK : nq_count_dihedral_resumable(N, rows, &cfg, ckpt, &total, &done,
+                                                                                    nullptr))
+                                    : nq_count_resumable(N, rows, &cfg, ckpt, &total, &done, nullptr);
+            if (dihedral && N < 4) done = 1;  // N = 2, 3: no solutions
             if (rc != NQ_OK) {
                 printf("n_queens_b200: %s (%s)\n", nq_status_string(rc), nq_last_error());
                 sum = -1;

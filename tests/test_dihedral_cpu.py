@@ -131,3 +131,31 @@ def test_every_orbit_gets_its_size(N):
             orbit = _images(q)
             seen |= orbit
             assert sum(weight[s] for s in orbit) == len(orbit), (N, k, q)
+
+
+def test_resumable_checkpoint_mode_is_checked(tmp_path):
+    # Read before any device work, so this runs without a GPU.
+    import ctypes
+    import struct
+    p = tmp_path / "ck"
+    t = ctypes.c_uint64(0)
+    d = ctypes.c_int(0)
+
+    def hdr(mode):
+        return b"NQB200CK" + struct.pack("<IiiiqqQQq", 1, 10, 3, mode, 100, 5, 7, 1, 0)
+
+    p.write_bytes(hdr(0))                                     # a plain count's checkpoint
+    assert nq.lib.nq_count_dihedral_resumable(10, 3, None, str(p).encode(), ctypes.byref(t), ctypes.byref(d),
+                                              None) == nq.NQ_ERR_ARG
+    assert "plain" in nq.last_error()
+    p.write_bytes(hdr(1))                                     # a dihedral count's checkpoint
+    assert nq.lib.nq_count_resumable(10, 3, None, str(p).encode(), ctypes.byref(t), ctypes.byref(d),
+                                     None) == nq.NQ_ERR_ARG
+    assert "dihedral" in nq.last_error()
+    p.write_bytes(hdr(2))                                     # unknown mode
+    assert nq.lib.nq_count_dihedral_resumable(10, 3, None, str(p).encode(), ctypes.byref(t), ctypes.byref(d),
+                                              None) == nq.NQ_ERR_ARG
+    one = b"NQB200CK" + struct.pack("<IiiiqqQQq", 1, 10, 3, 1, 100, 5, 7, 1, 1) + bytes(16)
+    p.write_bytes(one)                                        # an entry without its class byte
+    assert nq.lib.nq_count_dihedral_resumable(10, 3, None, str(p).encode(), ctypes.byref(t), ctypes.byref(d),
+                                              None) == nq.NQ_ERR_ARG

@@ -83,3 +83,42 @@ def test_cli_dihedral(gpu):
     exe = os.path.join(os.path.dirname(os.path.dirname(__file__)), "n_queens_b200", "n_queens")
     out = subprocess.run([exe, "16", "5", "--dihedral"], capture_output=True, text=True, timeout=120).stdout
     assert re.search(r"cuda 16 queens result 14772512, calc time", out), out
+
+
+# Resumable dihedral counts: every saved level keeps its class, so the count
+# is exact however often the kernel is stopped.
+@pytest.mark.parametrize("N,k,slice_ms", [(16, 5, 1), (17, 6, 1), (18, 6, 3), (19, 7, 15)])
+def test_sliced_dihedral_count_is_exact(gpu, tmp_path, N, k, slice_ms):
+    ck = str(tmp_path / f"d{N}.ckpt")
+    slices = 0
+    while True:
+        done, total, _ = gpu.count_resumable(N, k, ck, slice_ms=slice_ms, dihedral=True)
+        slices += 1
+        if done:
+            break
+        assert os.path.exists(ck) and not os.path.exists(ck + ".tmp")
+        assert slices < 3000
+    assert total == PUBLISHED[N]
+    assert slices >= 2, slices          # interrupted at least once
+    assert not os.path.exists(ck)
+
+
+def test_dihedral_and_plain_checkpoints_do_not_mix(gpu, tmp_path):
+    ck = str(tmp_path / "mix.ckpt")
+    done, _, _ = gpu.count_resumable(18, 6, ck, slice_ms=2, dihedral=True)
+    assert not done and os.path.exists(ck)
+    with pytest.raises(gpu.NQError):
+        gpu.count_resumable(18, 6, ck, slice_ms=2)
+    while not done:
+        done, total, _ = gpu.count_resumable(18, 6, ck, slice_ms=20, dihedral=True)
+    assert total == PUBLISHED[18]
+
+
+def test_cli_dihedral_checkpoint(gpu, tmp_path):
+    import subprocess
+    ck = str(tmp_path / "clid.ckpt")
+    out = subprocess.run([gpu.CLI_PATH, "18", "6", "--dihedral", "--checkpoint", ck, "--slice-ms", "5"],
+                         capture_output=True, text=True, timeout=600).stdout
+    assert "saved to" in out
+    assert "cuda 18 queens result 666090624, calc time: [" in out
+    assert not os.path.exists(ck)
