@@ -233,13 +233,15 @@ typedef struct nq_tune_entry {
     int split_rows;
     int block_threads;
     int layout;
-    double ms; /* mean graph replay time over `repeats` runs after one warm-up */
+    int inner_steps; /* DFS steps a warp runs between queue refills */
+    double ms;       /* mean graph replay time over `repeats` runs after one warm-up */
 } nq_tune_entry;
 
 /* Sweeps split depth 3..7, CTA size 64/128/256/512 and both stack layouts on
- * the given instances (other launch fields from `base`), replaying each
- * plan's graph; writes up to table_cap measured entries, their number and the
- * fastest. */
+ * the given instances (other launch fields from `base`), then queue chunking
+ * -- 256, 1024 (the default) and 4096 DFS steps between a warp's queue
+ * refills -- at the fastest of those; replays each plan's graph and writes up
+ * to table_cap measured entries (40 + 2), their number and the fastest. */
 int nq_batch_autotune(const nq_instance *inst, int64_t n, int repeats, const nq_config *base, nq_tune_entry *table,
                       int table_cap, int *n_entries, nq_tune_entry *best);
 

@@ -102,7 +102,7 @@ class TuneEntry(ctypes.Structure):
     """Mirror of ``nq_tune_entry``."""
 
     _fields_ = [("split_rows", ctypes.c_int), ("block_threads", ctypes.c_int), ("layout", ctypes.c_int),
-                ("ms", ctypes.c_double)]
+                ("inner_steps", ctypes.c_int), ("ms", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -437,7 +437,7 @@ class BatchPlan:
 
 
 def autotune_batch(instances, repeats: int = 2, config=None):
-    """Sweeps split depth, CTA size and stack layout; returns (best, table)."""
+    """Sweeps split depth, CTA size, stack layout and queue chunking; returns (best, table)."""
     arr, n = _instances(instances)
     table = (TuneEntry * 64)()
     cnt = ctypes.c_int(0)

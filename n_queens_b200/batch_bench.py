@@ -4,7 +4,7 @@ the top rows, seed 1 -- n_queens_b200.workloads.random_boards).
 
     python -m n_queens_b200.batch_bench [--tune-boards 512] [--repeats 3] [--json out.json]
 
-1. autotunes split depth / CTA size / stack layout (nq_batch_autotune) on a
+1. autotunes split depth / CTA size / stack layout / queue chunking (nq_batch_autotune) on a
    cheaper batch of the same shape (N in [12, 17], seed 2);
 2. builds the 4096-board plan with the winner and times graph replays;
 3. prints the plan's statistics and a checksum of the 4096 counts.
@@ -36,7 +36,8 @@ def main():
     boards = random_boards(4096, 1, 12, 20, 0, 4)
     t = time.perf_counter()
     plan = BatchPlan(boards, split_rows=best["split_rows"],
-                     config=dict(block_threads=best["block_threads"], layout=best["layout"]))
+                     config=dict(block_threads=best["block_threads"], layout=best["layout"],
+                                 inner_steps=best["inner_steps"]))
     build_s = time.perf_counter() - t
     runs = []
     out = None

@@ -1320,43 +1320,61 @@ int nq_batch_autotune(const nq_instance *inst, int64_t n, int repeats, const nq_
     static const int kSplits[] = {3, 4, 5, 6, 7};
     static const int kThreads[] = {64, 128, 256, 512};
     static const int kLayouts[] = {NQ_LAYOUT_INTERLEAVED, NQ_LAYOUT_LANE_MAJOR};
+    static const int kInner[] = {256, 4096};  // queue chunking tried beside the default
     nq_config cfg;
     if (base)
         cfg = *base;
     else
         memset(&cfg, 0, sizeof(cfg));
+    const int inner0 = cfg.inner_steps > 0 ? ((cfg.inner_steps + 3) & ~3) : kDefaultInner;
     int count = 0;
     best->ms = -1.0;
+    // Measures one configuration; NQ_ERR_DEPTH (the CTA cannot hold the
+    // stacks) skips it.
+    auto measure = [&](int split, int threads, int layout, int inner) -> int {
+        cfg.block_threads = threads;
+        cfg.layout = layout;
+        cfg.inner_steps = inner;
+        nq_batch *b = nullptr;
+        int rc = nq_batch_create(inst, n, split, &cfg, &b);
+        if (rc == NQ_ERR_DEPTH) return NQ_OK;
+        if (rc) return rc;
+        std::vector<uint64_t> outv((size_t)n);
+        nq_stats st;
+        rc = nq_batch_run(b, outv.data(), &st);  // warm-up
+        double sum_ms = 0;
+        for (int r = 0; r < repeats && rc == NQ_OK; ++r) {
+            rc = nq_batch_run(b, outv.data(), &st);
+            sum_ms += st.kernel_ms;
+        }
+        nq_batch_destroy(b);
+        if (rc) return rc;
+        nq_tune_entry e;
+        e.split_rows = split;
+        e.block_threads = threads;
+        e.layout = layout;
+        e.inner_steps = inner;
+        e.ms = sum_ms / repeats;
+        if (count < table_cap) table[count] = e;
+        ++count;
+        if (best->ms < 0 || e.ms < best->ms) *best = e;
+        return NQ_OK;
+    };
     for (int split : kSplits)
         for (int threads : kThreads)
             for (int layout : kLayouts) {
-                cfg.block_threads = threads;
-                cfg.layout = layout;
-                nq_batch *b = nullptr;
-                int rc = nq_batch_create(inst, n, split, &cfg, &b);
-                if (rc == NQ_ERR_DEPTH) continue;  // this CTA size cannot hold the stacks
+                const int rc = measure(split, threads, layout, inner0);
                 if (rc) return rc;
-                std::vector<uint64_t> outv((size_t)n);
-                nq_stats st;
-                rc = nq_batch_run(b, outv.data(), &st);  // warm-up
-                double sum_ms = 0;
-                for (int r = 0; r < repeats && rc == NQ_OK; ++r) {
-                    rc = nq_batch_run(b, outv.data(), &st);
-                    sum_ms += st.kernel_ms;
-                }
-                nq_batch_destroy(b);
-                if (rc) return rc;
-                nq_tune_entry e;
-                e.split_rows = split;
-                e.block_threads = threads;
-                e.layout = layout;
-                e.ms = sum_ms / repeats;
-                if (count < table_cap) table[count] = e;
-                ++count;
-                if (best->ms < 0 || e.ms < best->ms) *best = e;
             }
+    if (best->ms < 0) return NQ_ERR_ARG;
+    const nq_tune_entry first = *best;
+    for (int inner : kInner) {
+        if (inner == inner0) continue;
+        const int rc = measure(first.split_rows, first.block_threads, first.layout, inner);
+        if (rc) return rc;
+    }
     if (n_entries) *n_entries = count;
-    return best->ms < 0 ? NQ_ERR_ARG : NQ_OK;
+    return NQ_OK;
 }
 
 int nq_dihedral_expand(int N, int rows, uint32_t *cols, uint32_t *ld, uint32_t *rd, uint8_t *cls, int64_t cap,

@@ -205,12 +205,17 @@ def test_batch_autotune_sweep(gpu):
     inst = workloads.random_boards(96, 4, 9, 13, 0, 3)
     want = [oracle.count_task(*b) for b in inst]
     best, table = gpu.autotune_batch(inst, repeats=1)
-    assert len(table) == 40
+    assert len(table) == 42
     assert {e["split_rows"] for e in table} == {3, 4, 5, 6, 7}
     assert {e["block_threads"] for e in table} == {64, 128, 256, 512}
     assert {e["layout"] for e in table} == {0, 1}
+    assert {e["inner_steps"] for e in table} == {256, 1024, 4096}
+    # the chunking stage runs at the fastest entry of the first stage
+    first = min(table[:40], key=lambda e: e["ms"])
+    assert all((e["split_rows"], e["block_threads"], e["layout"]) ==
+               (first["split_rows"], first["block_threads"], first["layout"]) for e in table[40:])
     assert best["ms"] == min(e["ms"] for e in table)
-    cfg = dict(block_threads=best["block_threads"], layout=best["layout"])
+    cfg = dict(block_threads=best["block_threads"], layout=best["layout"], inner_steps=best["inner_steps"])
     assert gpu.count_batch(inst, split_rows=best["split_rows"], config=cfg).tolist() == want
 
 
