@@ -830,8 +830,10 @@ int count_resumable_impl(int N, int rows, const nq_config *cfg, const char *chec
         a.task_cls = (const uint8_t *)(d + 3 * n);
         rc = dih_upload_classes(c, N, rows, (size_t)n * 13, a);
         if (rc) return rc;
+        std::vector<DihClass> tab;
+        dihedral_classes(N, rows, tab);
         for (size_t i = 0; i < ncont; ++i)
-            if (ck.cls[i] >= kMaxDihClasses) {
+            if (ck.cls[i] >= tab.size()) {
                 g_last_error = "checkpoint holds a class index out of range";
                 return NQ_ERR_ARG;
             }

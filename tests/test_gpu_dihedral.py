@@ -122,3 +122,15 @@ def test_cli_dihedral_checkpoint(gpu, tmp_path):
     assert "saved to" in out
     assert "cuda 18 queens result 666090624, calc time: [" in out
     assert not os.path.exists(ck)
+
+
+def test_checkpoint_with_bad_class_index_is_refused(gpu, tmp_path):
+    ck = tmp_path / "bad.ckpt"
+    done, _, _ = gpu.count_resumable(18, 6, str(ck), slice_ms=2, dihedral=True)
+    assert not done
+    raw = bytearray(ck.read_bytes())
+    raw[-1] = 0xFF                       # the last saved level's class index
+    ck.write_bytes(bytes(raw))
+    with pytest.raises(gpu.NQError):
+        gpu.count_resumable(18, 6, str(ck), slice_ms=2, dihedral=True)
+    assert "class index" in gpu.last_error()
