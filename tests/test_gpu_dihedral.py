@@ -134,3 +134,11 @@ def test_checkpoint_with_bad_class_index_is_refused(gpu, tmp_path):
     with pytest.raises(gpu.NQError):
         gpu.count_resumable(18, 6, str(ck), slice_ms=2, dihedral=True)
     assert "class index" in gpu.last_error()
+
+
+@pytest.mark.parametrize("cfg", [dict(block_threads=32), dict(block_threads=512), dict(layout=1), dict(steal=-1),
+                                 dict(inner_steps=4), dict(inner_steps=8192), dict(stack_levels=25),
+                                 dict(blocks_per_sm=1)])
+def test_launch_shapes(gpu, cfg):
+    assert gpu.count_dihedral(16, 5, config=cfg).total == PUBLISHED[16]
+    assert gpu.count_dihedral(13, 3, config=cfg).total == PUBLISHED[13]
