@@ -7,7 +7,8 @@ Two ctypes libraries are exposed:
 
 * :data:`lib` -- ``liboracle_nq.so``, the plain-C restatement in
   ``nq_oracle.c`` (count, node count and expander, each citing the reference
-  line it restates);
+  line it restates) and ``dihedral_oracle.c`` (the 8-fold decomposition of the
+  library's dihedral entries, pinned by the reference's totals);
 * :func:`ref` -- ``_ref/libnq_ref.so``, the reference's own
   ``src/n_queens.cpp`` compiled unchanged behind ``ref_shim.cpp``.  It exists
   only where the reference sources were available at build time (the golden
