@@ -134,6 +134,16 @@ def test_cli_without_gpu():
                      out, re.M)
 
 
+@pytest.mark.skipif(not _no_gpu(), reason="checks the no-GPU path")
+def test_cli_dihedral_without_gpu(tmp_path):
+    ck = tmp_path / "d.ckpt"
+    for extra in ([], ["--checkpoint", str(ck), "--slice-ms", "5"]):
+        out = run_cli(12, 4, "--dihedral", *extra).stdout
+        assert "n_queens_b200: no CUDA device" in out
+        assert re.search(r"cuda 12 queens result -1, calc time: \[", out)
+    assert not ck.exists()
+
+
 def test_resumable_rejects_foreign_or_broken_checkpoints(tmp_path):
     # Checked before any device work, so this runs without a GPU.
     import struct
