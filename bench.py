@@ -82,6 +82,12 @@ def parse_args():
                     help="queue order of the headline arm; the other order is timed beside it")
     ap.add_argument("--no-compare", action="store_true", help="skip timing the other queue order")
     ap.add_argument("--no-dihedral", action="store_true", help="skip timing the dihedral decomposition")
+    ap.add_argument("--no-n22", action="store_true",
+                    help="skip the N=22 k=6 learned-vs-plain pair (run after the N=21 default workload)")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own GPU binary (oracle/_ref/n_queens_ref) on this GPU")
+    ap.add_argument("--no-build-e2e", action="store_true",
+                    help="skip the end-to-end learned count that includes building the cost model")
     return ap.parse_args()
 
 
@@ -144,7 +150,6 @@ def reference_sample(N: int, k: int, seconds: float, seed: int = 12345):
     `seconds` of the reference's CPU recursion on all host threads; returns
     (aos int32[n,3], nodes, counts, threads, kind)."""
     import oracle
-    from n_queens_b200 import workloads  # noqa: F401  (keeps the import surface uniform)
 
     cols, ld, rd = oracle.expand(N, k)
     rng = np.random.default_rng(seed)
@@ -172,6 +177,17 @@ def reference_sample(N: int, k: int, seconds: float, seed: int = 12345):
     cnt, nodes = oracle.count_tasks(N, cols[idx], ld[idx], rd[idx], nodes=True, threads=threads)
     aos = np.stack([cols[idx], ld[idx], rd[idx]], axis=1).view(np.int32)
     return aos, int(nodes.sum()), cnt, threads, kind
+
+
+def reference_sample_text(N, k, n, ntasks, nodes, threads, kind):
+    how = ("the reference's own n_queens() recursion (src/n_queens.cpp:8-21, compiled unchanged into "
+           "oracle/_ref/libnq_ref.so) called per task by the shim nqref_count_tasks with OpenMP "
+           f"schedule(dynamic,1) on {threads} threads -- not parallel_n_queens's hard-coded 32 threads with "
+           "static scheduling (src/n_queens.cpp:152-153)"
+           if kind == "reference" else
+           f"the C restatement of the reference recursion (oracle/nq_oracle.c) on {threads} threads")
+    return (f"{n} of {ntasks} N={N} k={k} prefix tasks (seeded uniform sample, {nodes} DFS nodes) through "
+            f"{how}, on {cpu_model()}")
 
 
 def time_reference(N, aos, threads, kind, cnt):
@@ -250,6 +266,66 @@ def traffic_from_profile(name: str):
     return None
 
 
+# ----------------------------------------------------------------------------- reference GPU binary
+def parse_reference_log(text: str):
+    """(start-job stamps, finish-job stamps, result, calc ms) from the
+    reference CLI's output: "[YYYY-mm-dd HH:MM:SS.mmm] " lines
+    (src/utils.cpp:14-30), "gpu [i] start job" / "gpu [i] finish job"
+    (src/n_queens_cuda.cu:154,178) and the result line (src/main.cpp:53)."""
+    import re
+
+    stamp = re.compile(r"^\[(\d{4}-\d\d-\d\d \d\d:\d\d:\d\d\.\d{3})\] (.*)$")
+
+    def when(t):
+        return datetime.datetime.strptime(t, "%Y-%m-%d %H:%M:%S.%f").timestamp()
+
+    starts, finishes, result, calc_ms = [], [], None, None
+    for line in text.splitlines():
+        m = stamp.match(line.strip())
+        if not m:
+            continue
+        body = m.group(2)
+        if "start job" in body:
+            starts.append(when(m.group(1)))
+        elif "finish job" in body:
+            finishes.append(when(m.group(1)))
+        rm = re.search(r"queens result (-?\d+), calc time: \[([0-9.]+)ms\]", body)
+        if rm:
+            result, calc_ms = int(rm.group(1)), float(rm.group(2))
+    return starts, finishes, result, calc_ms
+
+
+def reference_gpu_run(N: int, k: int, want: int, local: int) -> dict:
+    """The reference's own CLI + CUDA kernel (oracle/_ref/n_queens_ref: its
+    src/ files compiled unchanged for sm_100a, CONFIG2) on this rank's GPU,
+    one count per process (its queue word, src/n_queens_cuda.cu:8, is never
+    reset).  Job time = its "start job" to "finish job" log lines
+    (src/n_queens_cuda.cu:154,178); calc time = its own result line
+    (src/main.cpp:50-53), which also covers context creation and the host
+    expansion."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "n_queens_ref")
+    if not os.path.exists(exe):
+        return {"ran": False, "why": "oracle/_ref/n_queens_ref was not built (needs the reference sources)"}
+    env = dict(os.environ)
+    vis = env.get("CUDA_VISIBLE_DEVICES")
+    env["CUDA_VISIBLE_DEVICES"] = vis.split(",")[local] if vis else str(local)
+    t0 = time.perf_counter()
+    try:
+        p = subprocess.run([exe, str(N), str(k)], capture_output=True, text=True, env=env, timeout=900)
+    except subprocess.TimeoutExpired:
+        return {"ran": False, "why": "timed out after 900 s"}
+    wall = time.perf_counter() - t0
+    starts, finishes, result, calc_ms = parse_reference_log(p.stdout)
+    out = {"ran": True, "rc": p.returncode, "binary": "oracle/_ref/n_queens_ref (CONFIG2: 160 threads x 19 levels)",
+           "N": N, "k": k, "count": result, "count_ok": result == want, "calc_ms": calc_ms,
+           "process_wall_ms": 1000 * wall, "gpus_used": len(starts)}
+    if starts and finishes:
+        out["job_ms"] = 1000 * (max(finishes) - min(starts))
+    if result != want:
+        out["stdout_tail"] = p.stdout[-400:]
+    return out
+
+
 # ----------------------------------------------------------------------------- arms
 def run_reference(args, world, rank):
     wl = WORKLOADS[args.workload]
@@ -262,8 +338,7 @@ def run_reference(args, world, rank):
     times = [time_reference(N, aos, threads, kind, cnt) for _ in range(args.steps)]
     total = sum(times)
     value = nodes * args.steps / total
-    sample = (f"{aos.shape[0]} of {oracle_tasks(N, k)} N={N} k={k} prefix tasks (seeded uniform sample, "
-              f"{nodes} DFS nodes), reference n_queens() recursion, {threads} threads on {cpu_model()}")
+    sample = reference_sample_text(N, k, aos.shape[0], oracle_tasks(N, k), nodes, threads, kind)
     line = {
         "metric": METRIC, "value": value, "unit": "nodes/s", "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
@@ -400,40 +475,88 @@ def run_ours(args, world, rank, local):
                    "ms_per_step": 1000 * o_max / args.steps,
                    "headline_speedup": o_max / t_max}
 
-    # End to end through the public C ABI (nq_count): expansion, pinned H2D,
-    # kernel, D2H of the result words.
-    e2e = None
-    if not args.no_e2e:
+    # End to end through the public C ABI (nq_count_learned / nq_count):
+    # expansion, pinned H2D, schedule, kernel, D2H of the result words and of
+    # the per-CTA start/end stamps (nq_config.timing: makespan and tail idle).
+    def e2e_arm(kind, nsteps):
         ecfg = nq.Config()
         ecfg.device = local
+        ecfg.timing = 1
 
-        def e2e_count():
-            if head == "learned":
+        def one():
+            if kind == "learned":
                 return learned.count_learned(N, k, model, config=ecfg)
             return nq.count(N, k, config=ecfg)
 
-        r = e2e_count()  # sizes the library's buffers for this board
-        assert r.total == want
+        r = one()  # sizes the library's buffers for this board
+        if r.total != want:
+            raise SystemExit(f"e2e {kind}: count {r.total}, want {want}")
         barrier(world)
         walls, stats = [], []
-        for i in range(args.steps):
+        for i in range(nsteps):
             t0 = time.perf_counter()
-            r = e2e_count()
+            r = one()
             walls.append(time.perf_counter() - t0)
             if r.total != want:
-                raise SystemExit(f"e2e step {i}: count {r.total}, want {want}")
+                raise SystemExit(f"e2e {kind} step {i}: count {r.total}, want {want}")
             stats.append(r.stats)
         barrier(world)
         e_max = max_over_ranks(world, sum(walls))
-        e2e = {
-            "value": world * nodes * args.steps / e_max, "unit": "nodes/s",
-            "wall_ms_per_step": 1000 * e_max / args.steps,
-            "h2d_bytes_per_step": 12 * ntasks, "d2h_bytes_per_step": 24,
+        grid = int(stats[-1]["grid"])
+        return {
+            "value": world * nodes * nsteps / e_max, "unit": "nodes/s", "steps": nsteps,
+            "wall_ms_per_step": 1000 * e_max / nsteps,
+            "h2d_bytes_per_step": 12 * ntasks, "d2h_bytes_per_step": 24 + 16 * grid,
             "breakdown_ms": {key: statistics.mean(s[key] for s in stats)
                              for key in ("expand_ms", "h2d_ms", "schedule_ms", "kernel_ms", "d2h_ms", "total_ms")},
-            "api": "n_queens_b200.learned.count_learned (nq_count_learned)" if head == "learned"
+            "tail_idle_frac": statistics.mean(s["tail_idle_frac"] for s in stats),
+            "makespan_ms": statistics.mean(s["makespan_ms"] for s in stats),
+            "grid": grid, "block_threads": int(stats[-1]["block_threads"]),
+            "api": "n_queens_b200.learned.count_learned (nq_count_learned)" if kind == "learned"
                    else "n_queens_b200.count (nq_count)",
         }
+
+    e2e = e2e_other = None
+    if not args.no_e2e:
+        e2e = e2e_arm(head, args.steps)
+        if other:
+            e2e_other = e2e_arm(other, min(args.steps, 3))
+            e2e_other["schedule"] = other
+    if compare is not None and e2e is not None:
+        compare.update({
+            "makespan_ms": {head: e2e["makespan_ms"], other: e2e_other["makespan_ms"]},
+            "tail_idle_frac": {head: e2e["tail_idle_frac"], other: e2e_other["tail_idle_frac"]},
+            "e2e_wall_ms_per_step": {head: e2e["wall_ms_per_step"], other: e2e_other["wall_ms_per_step"]},
+            "note": "makespan and tail idle: per-CTA %globaltimer stamps of the e2e counts (nq_config.timing)"})
+
+    # The learned path with its model built inside the timed region: build
+    # (labels at N=16..18, pre-training, a labelled 5% fine-tuning sample and
+    # hold-out of this board), then the count of the tasks the build did not
+    # already count (nq_count_learned_reuse), against the plain e2e count.
+    build_e2e = None
+    if want_learned and not args.no_e2e and not args.no_build_e2e:
+        barrier(world)
+        t0 = time.perf_counter()
+        m2, rep2 = learned.build_cost_model(N, k=k, seed=2, device=local)
+        t_build = time.perf_counter() - t0
+        bcfg = nq.Config()
+        bcfg.device = local
+        bcfg.timing = 1
+        r = learned.count_learned(N, k, m2, config=bcfg, reuse=rep2)
+        wall = time.perf_counter() - t0
+        m2.close()
+        if r.total != want:
+            raise SystemExit(f"learned count with the model build: {r.total}, want {want}")
+        wall = max_over_ranks(world, wall)
+        plain_ms = e2e_other["wall_ms_per_step"] if (e2e_other and other == "plain") else (
+            e2e["wall_ms_per_step"] if head == "plain" else None)
+        build_e2e = {"wall_ms": 1000 * wall, "model_build_ms": 1000 * t_build,
+                     "count_wall_ms": 1000 * wall - 1000 * t_build, "kernel_ms": r.stats["kernel_ms"],
+                     "tasks_counted_by_build": int(rep2.counted_idx.size), "queue_tasks": int(ntasks - rep2.counted_idx.size),
+                     "count_ok": True, "plain_e2e_wall_ms": plain_ms,
+                     "speedup_vs_plain_e2e": (plain_ms / (1000 * wall)) if plain_ms else None,
+                     "api": "n_queens_b200.learned.build_cost_model + count_learned(reuse=...) "
+                            "(nq_count_learned_reuse)"}
 
     # The same count through the 8-fold decomposition (fewer nodes, same
     # total): wall and kernel time per count through nq_count_dihedral.
@@ -447,7 +570,8 @@ def run_ours(args, world, rank, local):
             raise SystemExit(f"dihedral: count {r.total}, want {want}")
         barrier(world)
         walls, kms = [], []
-        for i in range(args.steps):
+        dsteps = min(args.steps, 3)
+        for i in range(dsteps):
             t0 = time.perf_counter()
             r = nq.count_dihedral(N, kd, config=dcfg)
             walls.append(time.perf_counter() - t0)
@@ -456,10 +580,53 @@ def run_ours(args, world, rank, local):
             kms.append(r.stats["kernel_ms"])
         barrier(world)
         d_max = max_over_ranks(world, sum(walls))
-        dihedral = {"rows": kd, "tasks": int(r.stats["tasks"]), "count_ok": True,
-                    "wall_ms_per_step": 1000 * d_max / args.steps, "kernel_ms_per_step": statistics.mean(kms),
-                    "speedup_vs_headline_step": (1000 * t_max / args.steps) / (1000 * d_max / args.steps),
+        dihedral = {"rows": kd, "tasks": int(r.stats["tasks"]), "count_ok": True, "steps": dsteps,
+                    "wall_ms_per_step": 1000 * d_max / dsteps, "kernel_ms_per_step": statistics.mean(kms),
+                    "speedup_vs_headline_step": (1000 * t_max / args.steps) / (1000 * d_max / dsteps),
                     "api": "n_queens_b200.count_dihedral (nq_count_dihedral)"}
+
+    # The configuration the large-board target is quoted on: N=22, k=6,
+    # learned (model built once for N=22) then plain, each checked against the
+    # published total, with makespan and tail idle.
+    n22 = None
+    if args.workload == "n21k6" and not args.no_n22 and want_learned:
+        w22 = WORKLOADS["n22k6"]
+        barrier(world)
+        t0 = time.perf_counter()
+        m22, _ = learned.build_cost_model(22, k=6, seed=1, device=local)
+        b22 = time.perf_counter() - t0
+        runs = {}
+        for kind in ("learned", "plain"):
+            c22 = nq.Config()
+            c22.device = local
+            c22.timing = 1
+            barrier(world)
+            t0 = time.perf_counter()
+            r = learned.count_learned(22, 6, m22, config=c22) if kind == "learned" else nq.count(22, 6, config=c22)
+            wall = max_over_ranks(world, time.perf_counter() - t0)
+            if r.total != w22["total"]:
+                raise SystemExit(f"N=22 {kind}: count {r.total}, want {w22['total']}")
+            st = r.stats
+            runs[kind] = {"count": int(r.total), "count_ok": True, "tasks": int(st["tasks"]), "wall_ms": 1000 * wall,
+                          "kernel_ms": st["kernel_ms"], "schedule_ms": st["schedule_ms"],
+                          "makespan_ms": st["makespan_ms"], "tail_idle_frac": st["tail_idle_frac"],
+                          "block_threads": int(st["block_threads"]), "grid": int(st["grid"])}
+            if w22["nodes"]:
+                runs[kind]["nodes_per_s_kernel"] = w22["nodes"] / (st["kernel_ms"] / 1000.0)
+                runs[kind]["nodes_per_s_wall"] = world * w22["nodes"] / wall
+        m22.close()
+        n22 = {"N": 22, "k": 6, "tasks": runs["plain"]["tasks"], "count": w22["total"],
+               "dfs_nodes": w22["nodes"], "model_build_ms": 1000 * b22,
+               "learned": runs["learned"], "plain": runs["plain"],
+               "kernel_speedup_learned_over_plain": runs["plain"]["kernel_ms"] / runs["learned"]["kernel_ms"],
+               "wall_speedup_learned_over_plain": runs["plain"]["wall_ms"] / runs["learned"]["wall_ms"],
+               "api": "count_learned (nq_count_learned) then count (nq_count), nq_config.timing = 1"}
+
+    ref_gpu = None
+    if world == 1 and not args.no_reference_gpu:
+        ref_gpu = reference_gpu_run(N, k, want, local)
+        if ref_gpu.get("job_ms"):
+            ref_gpu["headline_step_speedup_vs_job"] = ref_gpu["job_ms"] / (1000 * t_max / args.steps)
 
     peak_clock = None
     try:
@@ -487,9 +654,7 @@ def run_ours(args, world, rank, local):
         aos, snodes, cnt, threads, kind = reference_sample(N, k, args.cpu_seconds)
         dt = time_reference(N, aos, threads, kind, cnt)
         cpu = {"value": snodes / dt, "unit": "nodes/s", "cores": threads, "kind": kind,
-               "sample": (f"{aos.shape[0]} of {ntasks} N={N} k={k} prefix tasks (seeded uniform sample, "
-                          f"{snodes} DFS nodes) through the reference n_queens() recursion, {threads} threads "
-                          f"on {cpu_model()}")}
+               "sample": reference_sample_text(N, k, aos.shape[0], ntasks, snodes, threads, kind)}
 
     if rank == 0:
         line = {
@@ -504,7 +669,8 @@ def run_ours(args, world, rank, local):
                        "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"replicas x{world}",
                        "stack_levels": levels},
             "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-            "compare": compare, "dihedral": dihedral, "model_build": build, "schedule_ms_per_step": sched_ms,
+            "compare": compare, "e2e_other": e2e_other, "build_e2e": build_e2e, "dihedral": dihedral,
+            "n22": n22, "reference_gpu": ref_gpu, "model_build": build, "schedule_ms_per_step": sched_ms,
             # our kernels per timed step: learned = predict + bin + DFS (the radix sort between
             # them is CUB's), plain = DFS
             "gpu_launches": sum(args.steps * (3 if a == "learned" else 1) for a in arms),

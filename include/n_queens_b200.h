@@ -63,7 +63,7 @@ enum { NQ_LAYOUT_INTERLEAVED = 0, NQ_LAYOUT_LANE_MAJOR = 1 };
 /* Launch parameters; zero-initialise and set what you need.  Zero means
  * "default" (the autotuned or built-in choice) for every field. */
 typedef struct nq_config {
-    int block_threads;      /* threads per CTA: 32..1024, multiple of 32; 0 = the size (64..256) that keeps
+    int block_threads;      /* threads per CTA: 32..1024, multiple of 32; 0 = the size (64..1024) that keeps
                                the most warps resident per SM for the launch's stack depth */
     int blocks_per_sm;      /* resident CTAs per SM for the persistent grid */
     int stack_levels;       /* per-lane DFS stack slots (>= N-1-rows)  */
@@ -79,7 +79,9 @@ typedef struct nq_config {
     int layout;             /* NQ_LAYOUT_INTERLEAVED (default) or NQ_LAYOUT_LANE_MAJOR */
     int device_expand;      /* nq_count: non-zero builds the prefix tasks on the device (nq_expand_device)
                                instead of on the host + H2D copy */
-    int reserved[3];
+    uint32_t queue_len;     /* queue positions to run, 0 = all n (must be <= n): the count covers only the
+                               tasks at positions 0 .. queue_len-1 (order[i] with NQ_ORDER_GIVEN, else i) */
+    int reserved[2];
 } nq_config;
 
 /* Timings and sizes of one call (all optional outputs). */
@@ -203,7 +205,10 @@ int nq_count_tasks_device(int N, const uint32_t *d_cols, const uint32_t *d_ld, c
  * control words first, so calls whose kernels overlap on the GPU race and
  * must be serialised by the caller.  The first call on a device performs the
  * device's set-up (the array's device address, the kernel's shared-memory
- * opt-in); make it before any stream capture. */
+ * opt-in); make it before any stream capture.  The launch shape (CTA size,
+ * DFS steps between queue visits, stack layout) is chosen from cfg exactly as
+ * nq_count_tasks_device chooses it, with the grid bounded by the array.  The
+ * caller's current device is the same after the call as before it. */
 int nq_count_tasks_device_noalloc(int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd,
                                   int64_t n, uint64_t *d_sum, const nq_config *cfg, void *stream);
 
@@ -294,10 +299,26 @@ int nq_mlp_train(nq_mlp *m, const uint8_t *task_n, const uint32_t *cols, const u
  * other entry of the same model before it has. */
 int nq_schedule_device(nq_mlp *m, int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd,
                        int64_t n, uint32_t *d_order, float *d_pred, void *stream);
+/* nq_schedule_device with the n_last tasks listed in d_last (device u32 task
+ * indices) placed behind every other task, in index order; an order run with
+ * nq_config.queue_len = n - n_last then skips exactly those tasks.  Indices
+ * at or beyond n are ignored.  No counterpart in the reference. */
+int nq_schedule_device_last(nq_mlp *m, int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd,
+                            int64_t n, const uint32_t *d_last, int64_t n_last, uint32_t *d_order, float *d_pred,
+                            void *stream);
 /* nq_count with the queue ordered by the model: expand, upload, schedule on
  * the device, count.  The same total as nq_count; stats->schedule_ms holds the
  * prediction + sort time.  The model must live on cfg->device. */
 int nq_count_learned(int N, int rows, nq_mlp *m, const nq_config *cfg, uint64_t *total, nq_stats *stats);
+/* nq_count_learned for a board part of whose tasks was already counted --
+ * typically the cost model's fine-tuning and hold-out samples, which the
+ * model build counts exactly to label them.  done_idx lists those task
+ * indices (expander order, ascending, distinct; n_done of them) and done_sum
+ * is the plain sum of their counts.  The queue holds only the other tasks,
+ * longest first, and *total = 2 x (done_sum + their sum), the same total as
+ * nq_count.  No counterpart in the reference. */
+int nq_count_learned_reuse(int N, int rows, nq_mlp *m, const int64_t *done_idx, int64_t n_done, uint64_t done_sum,
+                           const nq_config *cfg, uint64_t *total, nq_stats *stats);
 
 /* ---- Dihedral (8-fold) decomposition (no counterpart in the reference) ----
  * The reference counts only the left-right mirror: row 0 in the left half,

@@ -68,7 +68,8 @@ class Config(ctypes.Structure):
         ("timing", ctypes.c_int),
         ("layout", ctypes.c_int),
         ("device_expand", ctypes.c_int),
-        ("reserved", ctypes.c_int * 3),
+        ("queue_len", ctypes.c_uint32),
+        ("reserved", ctypes.c_int * 2),
     ]
 
 
@@ -196,7 +197,8 @@ EXPORTS = ("nq_abi_version", "nq_status_string", "nq_last_error", "nq_device_cou
            "nq_count_tasks", "nq_count_tasks_device", "nq_count_tasks_device_noalloc", "nq_count_batch",
            "nq_batch_create", "nq_batch_run", "nq_batch_destroy", "nq_batch_autotune",
            "nq_mlp_num_params", "nq_mlp_create", "nq_mlp_destroy", "nq_mlp_get_params", "nq_mlp_set_params",
-           "nq_mlp_predict", "nq_mlp_predict_tensor", "nq_mlp_grad", "nq_mlp_train", "nq_schedule_device", "nq_count_learned",
+           "nq_mlp_predict", "nq_mlp_predict_tensor", "nq_mlp_grad", "nq_mlp_train", "nq_schedule_device",
+           "nq_schedule_device_last", "nq_count_learned", "nq_count_learned_reuse",
            "nq_dihedral_expand", "nq_count_dihedral", "nq_count_dihedral_tasks",
            "nq_count_dihedral_resumable")
 

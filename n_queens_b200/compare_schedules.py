@@ -36,7 +36,8 @@ def main():
     if "learned" in names:
         t = time.perf_counter()
         model, rep = learned.build_cost_model(args.N, k=args.k, seed=args.seed)
-        out.update(model_build_s=time.perf_counter() - t, build=rep.__dict__)
+        out.update(model_build_s=time.perf_counter() - t,
+                   build={k: v for k, v in rep.__dict__.items() if k != "counted_idx"})
         print(json.dumps({"model_build_s": out["model_build_s"], "holdout_spearman": rep.holdout_spearman}),
               flush=True)
     for it in range(args.repeats):

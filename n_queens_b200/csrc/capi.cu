@@ -28,6 +28,7 @@
 #include "dfs_kernel.cuh"
 #include "dihedral.h"
 #include "expand.h"
+#include "launch.h"
 #include "n_queens_b200.h"
 
 namespace nqb {
@@ -36,8 +37,6 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 constexpr int kMaxBlocksPerSm = 32;
-constexpr int kDefaultThreads = 256;
-constexpr int kDefaultInner = 1024;
 // d_ctl layout (uint64 words): control words, results, per-CTA partials.
 constexpr int kWordSum = kCtlWords + 0;
 constexpr int kWordNodes = kCtlWords + 1;
@@ -65,33 +64,11 @@ double now_ms() {
 
 typedef void (*KernelFn)(DfsParams);
 
-// Step variant (see dfs_step): 0 = logic ops, unroll 4; 1 = pipe-balanced,
-// unroll 4; 2 = pipe-balanced, unroll 8.
-int g_variant = -1;
-
-int step_variant() {
-    if (g_variant < 0) {
-        const char *v = getenv("NQB_VARIANT");
-        g_variant = v ? atoi(v) : 2;
-        if (g_variant < 0 || g_variant > 2) g_variant = 2;
-    }
-    return g_variant;
-}
-
-template <bool PO, bool ND>
-KernelFn pick_variant(int v) {
-    switch (v) {
-        case 0: return dfs_kernel<PO, ND, 0, 4>;
-        case 1: return dfs_kernel<PO, ND, 1, 4>;
-        default: return dfs_kernel<PO, ND, 1, 8>;
-    }
-}
-
-KernelFn pick_kernel(bool per_owner, bool nodes, int v = -1, bool dih = false) {
-    if (dih) return per_owner ? dfs_kernel<true, false, 1, 8, false, true> : dfs_kernel<false, false, 1, 8, false, true>;
-    if (v < 0) v = step_variant();
-    if (per_owner) return nodes ? pick_variant<true, true>(v) : pick_variant<true, false>(v);
-    return nodes ? pick_variant<false, true>(v) : pick_variant<false, false>(v);
+KernelFn pick_kernel(bool per_owner, bool nodes, bool dih = false) {
+    if (dih) return per_owner ? dfs_kernel<true, false, 1, kUnroll, false, true>
+                              : dfs_kernel<false, false, 1, kUnroll, false, true>;
+    if (per_owner) return nodes ? dfs_kernel<true, true, 1, kUnroll> : dfs_kernel<true, false, 1, kUnroll>;
+    return nodes ? dfs_kernel<false, true, 1, kUnroll> : dfs_kernel<false, false, 1, kUnroll>;
 }
 
 struct DevBuf {
@@ -165,18 +142,17 @@ int ensure_ready(Ctx &c, int dev) {
     NQ_CUDA(cudaMalloc(&c.d_ctl, ctl_words * sizeof(unsigned long long)));
     NQ_CUDA(cudaMemset(c.d_ctl, 0, ctl_words * sizeof(unsigned long long)));
     // Dynamic shared memory above 48 KiB needs an opt-in per kernel.
-    const int static_smem = 2 * 32 * 8 + 16;
+    const int static_smem = kDfsStaticSmem;
     for (int po = 0; po < 2; ++po)
         for (int nd = 0; nd < 2; ++nd)
-            for (int v = 0; v < 3; ++v)
-                NQ_CUDA(cudaFuncSetAttribute(pick_kernel(po, nd, v), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             c.smem_optin - static_smem));
-    NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, 1, 8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 c.smem_optin - static_smem));
-    NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, 1, 8, true, true>,
+            NQ_CUDA(cudaFuncSetAttribute(pick_kernel(po, nd), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         c.smem_optin - static_smem));
+    NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, 1, kUnroll, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, c.smem_optin - static_smem));
+    NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, 1, kUnroll, true, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, c.smem_optin - static_smem));
     for (int po = 0; po < 2; ++po)
-        NQ_CUDA(cudaFuncSetAttribute(pick_kernel(po, false, -1, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
+        NQ_CUDA(cudaFuncSetAttribute(pick_kernel(po, false, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      c.smem_optin - static_smem));
     c.ready = true;
     return NQ_OK;
@@ -206,31 +182,9 @@ struct Launch {
 };
 
 // Chooses the persistent grid: CTA size, stack slots per lane and as many
-// resident CTAs per SM as shared memory and registers allow.
-// Default CTA size: the one that keeps the most warps resident per SM for
-// this stack depth (each warp's stack is levels x 512 B of shared memory, so
-// CTA granularity decides how much of it can be used), the larger CTA on a
-// tie.  N=21 (14 levels): 256 threads fit 24 warps, 192 fit 30 -- 6 % faster.
-int best_threads(Ctx &c, KernelFn fn, int levels, int cap_per_sm) {
-    const int static_smem = 2 * 32 * 8 + 16;
-    int best = kDefaultThreads, best_warps = 0;
-    for (int t = kDefaultThreads; t >= 64; t -= 32) {
-        const int smem = (t / 32) * levels * (int)kSlotBytes;
-        if (smem + static_smem > c.smem_optin) continue;
-        int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, t, smem) != cudaSuccess) {
-            (void)cudaGetLastError();
-            continue;
-        }
-        per_sm = std::min(per_sm, cap_per_sm);
-        if (per_sm * (t / 32) > best_warps) {
-            best_warps = per_sm * (t / 32);
-            best = t;
-        }
-    }
-    return best;
-}
-
+// resident CTAs per SM as shared memory and registers allow.  Default CTA
+// size: resident_warp_threads (launch.h), the one that keeps the most warps
+// resident per SM for this stack depth.
 int plan_launch(Ctx &c, const nq_config *cfg, int levels_needed, bool per_owner, bool nodes, Launch &L,
                 bool dih = false) {
     L.dih = dih;
@@ -246,19 +200,22 @@ int plan_launch(Ctx &c, const nq_config *cfg, int levels_needed, bool per_owner,
                                                            : kMaxBlocksPerSm;
     L.threads = (cfg && cfg->block_threads)
                     ? cfg->block_threads
-                    : best_threads(c, pick_kernel(per_owner, nodes, -1, dih), L.levels, cap_per_sm);
+                    : resident_warp_threads(pick_kernel(per_owner, nodes, dih), L.levels, c.smem_optin, cap_per_sm);
+    if (!(cfg && cfg->block_threads) && L.threads == 0) {
+        g_last_error = "no CTA size of 64 or more threads fits this stack depth in shared memory";
+        return NQ_ERR_DEPTH;
+    }
     if (L.threads < 32 || L.threads > 1024 || (L.threads & 31)) {
         g_last_error = "block_threads must be a multiple of 32 in [32, 1024]";
         return NQ_ERR_ARG;
     }
     L.smem = (L.threads / 32) * L.levels * (int)kSlotBytes;
-    const int static_smem = 2 * 32 * 8 + 16;
-    if (L.smem + static_smem > c.smem_optin) {
+    if (L.smem + kDfsStaticSmem > c.smem_optin) {
         g_last_error = "per-CTA stack does not fit in shared memory: lower block_threads";
         return NQ_ERR_DEPTH;
     }
     int per_sm = 0;
-    NQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_kernel(per_owner, nodes, -1, dih),
+    NQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_kernel(per_owner, nodes, dih),
                                                           L.threads, L.smem));
     if (per_sm <= 0) {
         g_last_error = "launch configuration cannot be resident";
@@ -289,7 +246,7 @@ int enqueue_dfs(Ctx &c, DfsParams p, const Launch &L, bool per_owner, bool nodes
     p.layout = L.layout;
     NQ_CUDA(cudaMemsetAsync(p.ctl, 0, kCtlWords * sizeof(unsigned long long), s));
     if (p.cta_times) NQ_CUDA(cudaMemsetAsync(p.cta_times, 0, 2 * (size_t)L.grid * sizeof(unsigned long long), s));
-    pick_kernel(per_owner, nodes, -1, L.dih)<<<L.grid, L.threads, L.smem, s>>>(p);
+    pick_kernel(per_owner, nodes, L.dih)<<<L.grid, L.threads, L.smem, s>>>(p);
     NQ_CUDA(cudaGetLastError());
     return NQ_OK;
 }
@@ -311,6 +268,19 @@ DfsParams base_params(Ctx &c, int N, int64_t n, const nq_config *cfg) {
     p.block_nodes = c.d_ctl + kWordBlocks + (size_t)c.sms * kMaxBlocksPerSm;
     if (cfg && cfg->timing) p.cta_times = c.d_ctl + kWordBlocks + 2 * (size_t)c.sms * kMaxBlocksPerSm;
     return p;
+}
+
+// Queue length of a launch over n tasks: cfg->queue_len positions, or all.
+int queue_len_of(const nq_config *cfg, int64_t n, long long &q) {
+    q = n;
+    if (cfg && cfg->queue_len) {
+        if ((int64_t)cfg->queue_len > n) {
+            g_last_error = "queue_len exceeds the number of tasks";
+            return NQ_ERR_ARG;
+        }
+        q = (long long)cfg->queue_len;
+    }
+    return NQ_OK;
 }
 
 int status_from_bits(unsigned long long bits) {
@@ -366,13 +336,30 @@ struct DihArgs {
 int count_resident(Ctx &c, int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd, int64_t n,
                    int levels_needed, const nq_config *cfg, bool per_owner, bool nodes, uint64_t *h_per_task,
                    uint64_t *h_nodes_task, uint64_t *sum, uint64_t *nodes_total, nq_stats *st, bool timed_h2d,
-                   const uint32_t *d_order = nullptr, const DihArgs *dih = nullptr) {
+                   const uint32_t *d_order = nullptr, const DihArgs *dih = nullptr, int64_t nqueue = -1) {
     if (dih) nodes = false;
     Launch L;
     int rc = plan_launch(c, cfg, levels_needed, per_owner, nodes, L, dih != nullptr);
     if (rc) return rc;
     fill_stats_launch(st, L);
     DfsParams p = base_params(c, N, n, cfg);
+    long long qlen = n;
+    if (nqueue >= 0) {
+        qlen = nqueue;  // the caller's internal order decides the queue
+    } else {
+        rc = queue_len_of(cfg, n, qlen);
+        if (rc) return rc;
+    }
+    p.nqueue = qlen;
+    if (qlen == 0 && n > 0) {
+        // nothing queued: no launch, the sum is 0
+        if (sum) *sum = 0;
+        if (nodes_total) *nodes_total = 0;
+        if (per_owner && h_per_task) memset(h_per_task, 0, (size_t)n * 8);
+        if (per_owner && nodes && h_nodes_task) memset(h_nodes_task, 0, (size_t)n * 8);
+        if (st) st->kernel_ms = 0;
+        return NQ_OK;
+    }
     p.cols = d_cols;
     p.ld = d_ld;
     p.rd = d_rd;
@@ -844,7 +831,7 @@ int count_resumable_impl(int N, int rows, const nq_config *cfg, const char *chec
         NQ_CUDA(cudaMemcpyAsync(d_cont_in, ck.cont.data(), ncont * 16, cudaMemcpyHostToDevice, c.stream));
         if (dih) NQ_CUDA(cudaMemcpyAsync(d_cont_cls, ck.cls.data(), ncont, cudaMemcpyHostToDevice, c.stream));
     }
-    KernelFn fn = dih ? dfs_kernel<false, false, 1, 8, true, true> : dfs_kernel<false, false, 1, 8, true>;
+    KernelFn fn = dih ? dfs_kernel<false, false, 1, kUnroll, true, true> : dfs_kernel<false, false, 1, kUnroll, true>;
     Launch L;
     rc = plan_launch(c, cfg, N - 1 - rows, false, false, L, dih);
     if (rc) return rc;
@@ -1110,10 +1097,20 @@ int nq_count_dihedral_resumable(int N, int rows, const nq_config *cfg, const cha
     return count_resumable_impl(N, rows, cfg, checkpoint_path, true, total, done, stats);
 }
 
-int nq_count_learned(int N, int rows, nq_mlp *m, const nq_config *cfg, uint64_t *total, nq_stats *stats) {
+}  // extern "C"
+
+namespace nqb {
+namespace {
+
+// nq_count_learned and nq_count_learned_reuse: expand, upload, order the
+// queue longest-first on the device (the listed already-counted tasks last,
+// outside the queue), count.
+int count_learned_impl(int N, int rows, nq_mlp *m, const int64_t *done_idx, int64_t n_done, uint64_t done_sum,
+                       const nq_config *cfg, uint64_t *total, nq_stats *stats) {
     const double t0 = now_ms();
     if (stats) memset(stats, 0, sizeof(*stats));
     if (N < 2 || N > NQ_MAX_N || rows < 1 || rows > N - 2 || !total || !m) return NQ_ERR_ARG;
+    if (n_done < 0 || (n_done > 0 && !done_idx)) return NQ_ERR_ARG;
     Ctx *cp = nullptr;
     int rc = lock_device(device_of(cfg), cp);
     if (rc) return rc;
@@ -1127,7 +1124,8 @@ int nq_count_learned(int N, int rows, nq_mlp *m, const nq_config *cfg, uint64_t 
     const int64_t n = expand_prefixes_to(
         N, rows,
         [&](int64_t total_tasks, uint32_t **pc, uint32_t **pl, uint32_t **pr, int64_t *cap) {
-            grow_rc = c.h_tasks.grow((size_t)std::max<int64_t>(total_tasks, 1) * 12);
+            // tasks (12 B each), then the already-counted indices (4 B each)
+            grow_rc = c.h_tasks.grow((size_t)std::max<int64_t>(total_tasks, 1) * 12 + (size_t)n_done * 4 + 256);
             if (grow_rc) return false;
             h = (uint32_t *)c.h_tasks.p;
             *pc = h;
@@ -1139,22 +1137,38 @@ int nq_count_learned(int N, int rows, nq_mlp *m, const nq_config *cfg, uint64_t 
         0);
     if (grow_rc) return grow_rc;
     if (n < 0 || n > 0xffffffffll) return NQ_ERR_ARG;
+    if (n_done > n) {
+        g_last_error = "more already-counted tasks than the board has";
+        return NQ_ERR_ARG;
+    }
+    // The listed indices must be distinct and in range: ascending order is
+    // required, so one pass checks both.
+    uint32_t *h_done = h + 3 * n;
+    for (int64_t i = 0; i < n_done; ++i) {
+        if (done_idx[i] < 0 || done_idx[i] >= n || (i > 0 && done_idx[i] <= done_idx[i - 1])) {
+            g_last_error = "already-counted task indices must be ascending, distinct and below the task count";
+            return NQ_ERR_ARG;
+        }
+        h_done[i] = (uint32_t)done_idx[i];
+    }
     if (stats) {
         stats->expand_ms = now_ms() - te;
         stats->tasks = n;
     }
-    // tasks (12 B each) followed by the order (4 B each)
-    rc = c.tasks.grow((size_t)std::max<int64_t>(n, 1) * 16 + 256);
+    // tasks (12 B each), the order (4 B each), the already-counted indices
+    rc = c.tasks.grow((size_t)std::max<int64_t>(n, 1) * 16 + (size_t)n_done * 4 + 256);
     if (rc) return rc;
     uint32_t *d = (uint32_t *)c.tasks.p;
     uint32_t *d_order = d + 3 * n;
+    uint32_t *d_done = d + 4 * n;
     NQ_CUDA(cudaEventRecord(c.ev[0], c.stream));
     if (n) NQ_CUDA(cudaMemcpyAsync(d, h, (size_t)n * 12, cudaMemcpyHostToDevice, c.stream));
+    if (n_done) NQ_CUDA(cudaMemcpyAsync(d_done, h_done, (size_t)n_done * 4, cudaMemcpyHostToDevice, c.stream));
     cudaEvent_t e_sched0 = nullptr, e_sched1 = nullptr;
     NQ_CUDA(cudaEventCreate(&e_sched0));
     NQ_CUDA(cudaEventCreate(&e_sched1));
     NQ_CUDA(cudaEventRecord(e_sched0, c.stream));
-    rc = nq_schedule_device(m, N, d, d + n, d + 2 * n, n, d_order, nullptr, c.stream);
+    rc = nq_schedule_device_last(m, N, d, d + n, d + 2 * n, n, d_done, n_done, d_order, nullptr, c.stream);
     if (rc) {
         cudaEventDestroy(e_sched0);
         cudaEventDestroy(e_sched1);
@@ -1163,7 +1177,7 @@ int nq_count_learned(int N, int rows, nq_mlp *m, const nq_config *cfg, uint64_t 
     NQ_CUDA(cudaEventRecord(e_sched1, c.stream));
     uint64_t sum = 0;
     rc = count_resident(c, N, d, d + n, d + 2 * n, n, N - 1 - rows, cfg, false, false, nullptr, nullptr, &sum,
-                        nullptr, stats, true, d_order);
+                        nullptr, stats, true, d_order, nullptr, n - n_done);
     if (stats) {
         float ms = 0;
         cudaEventElapsedTime(&ms, e_sched0, e_sched1);
@@ -1174,8 +1188,24 @@ int nq_count_learned(int N, int rows, nq_mlp *m, const nq_config *cfg, uint64_t 
     }
     cudaEventDestroy(e_sched0);
     cudaEventDestroy(e_sched1);
-    *total = 2 * sum;
+    // The reference doubles every per-prefix sum for the mirror image
+    // (src/n_queens_cuda.cu:181-183).
+    *total = 2 * (sum + done_sum);
     return rc;
+}
+
+}  // namespace
+}  // namespace nqb
+
+extern "C" {
+
+int nq_count_learned(int N, int rows, nq_mlp *m, const nq_config *cfg, uint64_t *total, nq_stats *stats) {
+    return count_learned_impl(N, rows, m, nullptr, 0, 0, cfg, total, stats);
+}
+
+int nq_count_learned_reuse(int N, int rows, nq_mlp *m, const int64_t *done_idx, int64_t n_done, uint64_t done_sum,
+                           const nq_config *cfg, uint64_t *total, nq_stats *stats) {
+    return count_learned_impl(N, rows, m, done_idx, n_done, done_sum, cfg, total, stats);
 }
 
 int nq_count_tasks(int N, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd, int64_t n,
@@ -1245,6 +1275,10 @@ int nq_count_tasks_device(int N, const uint32_t *d_cols, const uint32_t *d_ld, c
     rc = plan_launch(c, cfg, need, per_owner, want_nodes, L);
     if (rc) return rc;
     DfsParams p = base_params(c, N, n, cfg);
+    long long qlen = n;
+    rc = queue_len_of(cfg, n, qlen);
+    if (rc) return rc;
+    p.nqueue = qlen;
     p.cols = d_cols;
     p.ld = d_ld;
     p.rd = d_rd;

@@ -62,6 +62,7 @@ struct DfsParams {
     const uint32_t *owner_of;  // per-task output slot, or nullptr (slot = task index)
     const uint32_t *order;     // queue position -> task index, or nullptr (identity)
     long long ntasks;
+    long long nqueue;          // queue positions to run (<= ntasks; 0 = ntasks)
     int N;                     // board size when task_n is nullptr
     int levels;                // stack slots per lane
     int inner;                 // DFS steps per outer trip (multiple of 4)
@@ -354,7 +355,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
     uint32_t owner = kNoOwner;
     DihLane dih;
     unsigned long long tot = 0, tot_nodes = 0;
-    const long long qlen = RESUME ? p.n_cont_in + p.ntasks - p.task_base : p.ntasks;
+    const long long qlen = RESUME ? p.n_cont_in + p.ntasks - p.task_base : (p.nqueue > 0 ? p.nqueue : p.ntasks);
     bool queue_live = qlen > 0;
     bool timed_out = false;
     unsigned long long deadline = 0;

@@ -587,12 +587,23 @@ __global__ void mlp_adam_kernel(float *master, float *m1, float *m2, const float
     }
 }
 
-// Sort keys for the longest-first order: predicted log2 cost in 1/8 units.
+// Sort keys for the longest-first order: 1 + predicted log2 cost in 1/8
+// units (key 0 is kept for tasks that must go last, mlp_last_kernel).
 __global__ void mlp_bin_kernel(const float *pred, long long n, uint16_t *key, uint32_t *idx) {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        const float v = fminf(fmaxf(pred[t] * 8.f + 0.5f, 0.f), 65535.f);
-        key[t] = (uint16_t)v;
+        const float v = fminf(fmaxf(pred[t] * 8.f + 0.5f, 0.f), 65534.f);
+        key[t] = (uint16_t)(1.f + v);
         idx[t] = (uint32_t)t;
+    }
+}
+
+// Moves the listed tasks behind every other task of the order (key 0).
+// Indices at or beyond n are ignored.
+__global__ void mlp_last_kernel(const uint32_t *last, long long n_last, long long n, uint16_t *key) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_last;
+         i += (long long)gridDim.x * blockDim.x) {
+        const uint32_t t = last[i];
+        if ((long long)t < n) key[t] = 0;
     }
 }
 
@@ -959,12 +970,14 @@ int nq_mlp_train(nq_mlp *m, const uint8_t *task_n, const uint32_t *cols, const u
 
 // Longest-first order of device-resident tasks: predictions -> keys in
 // 1/8-log2 bins -> stable descending radix sort of task indices.
-int nq_schedule_device(nq_mlp *m, int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd,
-                       int64_t n, uint32_t *d_order, float *d_pred, void *stream) {
+int nq_schedule_device_last(nq_mlp *m, int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd,
+                            int64_t n, const uint32_t *d_last, int64_t n_last, uint32_t *d_order, float *d_pred,
+                            void *stream) {
     int rc = check_model(m);
     if (rc) return rc;
     if (N < 1 || N > NQ_MAX_N || n < 0 || n > 0xffffffffll || (n > 0 && (!d_cols || !d_ld || !d_rd || !d_order)))
         return NQ_ERR_ARG;
+    if (n_last < 0 || (n_last > 0 && !d_last)) return NQ_ERR_ARG;
     if (n == 0) return NQ_OK;
     std::lock_guard<std::mutex> lock(m->mu);
     cudaStream_t s = (cudaStream_t)stream;  // NULL: the legacy default stream, as in every device entry
@@ -981,12 +994,21 @@ int nq_schedule_device(nq_mlp *m, int N, const uint32_t *d_cols, const uint32_t 
     if (rc) return rc;
     mlp_bin_kernel<<<m->sms * 4, 256, 0, s>>>(pred, n, key, idx);
     MLP_CUDA(cudaGetLastError());
+    if (n_last > 0) {
+        mlp_last_kernel<<<m->sms * 4, 256, 0, s>>>(d_last, n_last, n, key);
+        MLP_CUDA(cudaGetLastError());
+    }
     size_t tmp = 0;
     MLP_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, key, key2, idx, d_order, (int)n, 0, 16, s));
     rc = grow(m->sort_tmp, m->sort_tmp_cap, tmp);
     if (rc) return rc;
     MLP_CUDA(cub::DeviceRadixSort::SortPairsDescending(m->sort_tmp, tmp, key, key2, idx, d_order, (int)n, 0, 16, s));
     return NQ_OK;
+}
+
+int nq_schedule_device(nq_mlp *m, int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd,
+                       int64_t n, uint32_t *d_order, float *d_pred, void *stream) {
+    return nq_schedule_device_last(m, N, d_cols, d_ld, d_rd, n, nullptr, 0, d_order, d_pred, stream);
 }
 
 }  // extern "C"

@@ -30,6 +30,7 @@
 #include <string>
 
 #include "dfs_kernel.cuh"
+#include "launch.h"
 #include "n_queens_b200.h"
 
 namespace nqb {
@@ -42,7 +43,7 @@ namespace {
 constexpr int kNoAllocMaxCtas = 8192;
 constexpr int kNoAllocWords = 8 + kNoAllocMaxCtas;  // control + results + per-CTA partials
 constexpr int kNoAllocMaxDevices = 64;
-constexpr int kNoAllocThreads = 256;
+constexpr int kNoAllocMaxBlocksPerSm = 32;
 
 // The scratch itself.  In host code `g_noalloc_scratch` is only a host-side
 // stand-in for the device symbol: its device address comes from
@@ -60,12 +61,52 @@ std::mutex g_noalloc_mu;
 NoAllocDev g_noalloc_dev[kNoAllocMaxDevices];
 
 typedef void (*NoAllocKernel)(DfsParams);
-NoAllocKernel noalloc_kernel() { return dfs_kernel<false, false, 1, 8>; }
+// The same instantiation the allocating device entry runs for a plain count.
+NoAllocKernel noalloc_kernel() { return dfs_kernel<false, false, 1, kUnroll>; }
 
 int noalloc_fail(cudaError_t e, const char *what) {
     set_last_error((std::string(what) + ": " + cudaGetErrorString(e)).c_str());
     (void)cudaGetLastError();
     return NQ_ERR_CUDA;
+}
+
+// Puts the caller's current device back when the entry returns, so a host
+// framework that keeps its own notion of the current device never sees it
+// change.
+struct CurrentDeviceGuard {
+    int saved = -1;
+    ~CurrentDeviceGuard() {
+        if (saved >= 0) cudaSetDevice(saved);
+    }
+};
+
+// The device checks of the other entries: a device must exist, the ordinal
+// must be in range, and the device must be an sm_100 part (the library
+// carries only an sm_100a image).
+int noalloc_check_device(int dev) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        (void)cudaGetLastError();
+        set_last_error("no CUDA device");
+        return NQ_ERR_NO_DEVICE;
+    }
+    if (dev < 0 || dev >= n || dev >= kNoAllocMaxDevices) {
+        set_last_error("device ordinal out of range");
+        return NQ_ERR_ARG;
+    }
+    int major = 0, minor = 0;
+    e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (e != cudaSuccess) return noalloc_fail(e, "cudaDeviceGetAttribute");
+    e = cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+    if (e != cudaSuccess) return noalloc_fail(e, "cudaDeviceGetAttribute");
+    if (major != 10 || minor != 0) {
+        set_last_error(("device is sm_" + std::to_string(major) + std::to_string(minor) +
+                        "; this library carries only an sm_100a image")
+                           .c_str());
+        return NQ_ERR_NO_KERNEL;
+    }
+    return NQ_OK;
 }
 
 // Once per device, with that device current.
@@ -77,9 +118,8 @@ int noalloc_setup(int dev, NoAllocDev &d) {
     if (e != cudaSuccess) return noalloc_fail(e, "cudaDeviceGetAttribute");
     e = cudaDeviceGetAttribute(&d.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return noalloc_fail(e, "cudaDeviceGetAttribute");
-    const int static_smem = 2 * 32 * 8 + 16;
     e = cudaFuncSetAttribute(noalloc_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             d.smem_optin - static_smem);
+                             d.smem_optin - kDfsStaticSmem);
     if (e != cudaSuccess) return noalloc_fail(e, "cudaFuncSetAttribute");
     d.ready = true;
     return NQ_OK;
@@ -96,46 +136,60 @@ extern "C" int nq_count_tasks_device_noalloc(int N, const uint32_t *d_cols, cons
     if (N < 1 || N > NQ_MAX_N || n < 0 || n > 0xffffffffll || !d_sum) return NQ_ERR_ARG;
     if (n > 0 && (!d_cols || !d_ld || !d_rd)) return NQ_ERR_ARG;
     const int dev = cfg ? cfg->device : 0;
-    if (dev < 0 || dev >= kNoAllocMaxDevices) return NQ_ERR_ARG;
-    int cur = -1;
-    cudaError_t e = cudaGetDevice(&cur);
+    int rc = noalloc_check_device(dev);
+    if (rc) return rc;
+    CurrentDeviceGuard guard;
+    cudaError_t e = cudaGetDevice(&guard.saved);
     if (e != cudaSuccess) return noalloc_fail(e, "cudaGetDevice");
-    if (cur != dev) {
+    if (guard.saved != dev) {
         e = cudaSetDevice(dev);
         if (e != cudaSuccess) return noalloc_fail(e, "cudaSetDevice");
+    } else {
+        guard.saved = -1;  // nothing to restore
     }
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     NoAllocDev &d = g_noalloc_dev[dev];
-    int rc = noalloc_setup(dev, d);
+    rc = noalloc_setup(dev, d);
     if (rc) return rc;
     if (d.sms > kNoAllocMaxCtas) {
         set_last_error("this GPU has more SMs than the fixed scratch array has CTA slots");
         return NQ_ERR_ARG;
     }
+    if (cfg && cfg->blocks_per_sm > 0 && (long long)cfg->blocks_per_sm * d.sms > kNoAllocMaxCtas) {
+        set_last_error(("blocks_per_sm x SMs exceeds the " + std::to_string(kNoAllocMaxCtas) +
+                        " CTAs that the fixed scratch array can hold")
+                           .c_str());
+        return NQ_ERR_ARG;
+    }
 
-    // Launch shape: as in the other entries, but the grid must fit the
-    // array's per-CTA partials.
-    const int threads = (cfg && cfg->block_threads) ? cfg->block_threads : kNoAllocThreads;
-    if (threads < 32 || threads > 1024 || (threads & 31)) return NQ_ERR_ARG;
+    // Launch shape: chosen exactly as the allocating entries choose it (the
+    // CTA size that keeps the most warps resident for the stack depth, 1024
+    // DFS steps between queue visits), with the grid bounded by the array's
+    // per-CTA partials.
     const int levels = (cfg && cfg->stack_levels > 0) ? cfg->stack_levels : std::max(1, N - 1);
+    int cap_per_sm = std::min(kNoAllocMaxBlocksPerSm, std::max(1, kNoAllocMaxCtas / d.sms));
+    if (cfg && cfg->blocks_per_sm > 0) cap_per_sm = std::min(cap_per_sm, cfg->blocks_per_sm);
+    const int threads = (cfg && cfg->block_threads)
+                            ? cfg->block_threads
+                            : resident_warp_threads(noalloc_kernel(), levels, d.smem_optin, cap_per_sm);
+    if (threads == 0) {
+        set_last_error("no CTA size of 64 or more threads fits this stack depth in shared memory");
+        return NQ_ERR_DEPTH;
+    }
+    if (threads < 32 || threads > 1024 || (threads & 31)) return NQ_ERR_ARG;
     const int smem = (threads / 32) * levels * (int)kSlotBytes;
-    if (smem + 2 * 32 * 8 + 16 > d.smem_optin) {
+    if (smem + kDfsStaticSmem > d.smem_optin) {
         set_last_error("per-CTA stack does not fit in shared memory: lower block_threads or stack_levels");
         return NQ_ERR_DEPTH;
     }
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, noalloc_kernel(), threads, smem);
     if (e != cudaSuccess) return noalloc_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    if (per_sm <= 0) return NQ_ERR_ARG;
-    if (cfg && cfg->blocks_per_sm > 0) {
-        if ((long long)cfg->blocks_per_sm * d.sms > kNoAllocMaxCtas) {
-            set_last_error(("blocks_per_sm x SMs exceeds the " + std::to_string(kNoAllocMaxCtas) +
-                            " CTAs that the fixed scratch array can hold").c_str());
-            return NQ_ERR_ARG;
-        }
-        per_sm = std::min(per_sm, cfg->blocks_per_sm);
+    if (per_sm <= 0) {
+        set_last_error("launch configuration cannot be resident");
+        return NQ_ERR_ARG;
     }
-    per_sm = std::min(per_sm, std::max(1, kNoAllocMaxCtas / d.sms));
+    per_sm = std::min(per_sm, cap_per_sm);
     const int grid = d.sms * per_sm;
 
     DfsParams p;
@@ -144,24 +198,33 @@ extern "C" int nq_count_tasks_device_noalloc(int N, const uint32_t *d_cols, cons
     p.ld = d_ld;
     p.rd = d_rd;
     p.ntasks = n;
+    if (cfg && cfg->queue_len) {
+        if ((int64_t)cfg->queue_len > n) {
+            set_last_error("queue_len exceeds the number of tasks");
+            return NQ_ERR_ARG;
+        }
+        p.nqueue = (long long)cfg->queue_len;
+    }
     p.N = N;
     p.levels = levels;
-    p.inner = (cfg && cfg->inner_steps > 0) ? ((cfg->inner_steps + 3) & ~3) : 256;
+    p.inner = (cfg && cfg->inner_steps > 0) ? ((cfg->inner_steps + 3) & ~3) : kDefaultInner;
     p.steal = (cfg && cfg->steal < 0) ? 0 : 1;
+    p.layout = (cfg && cfg->layout == NQ_LAYOUT_LANE_MAJOR) ? 1 : 0;
     p.limit_ns = cfg ? (unsigned long long)cfg->time_limit_ms * 1000000ull : 0ull;
     p.order = (cfg && cfg->order_kind == NQ_ORDER_GIVEN) ? cfg->order : nullptr;
-    p.ctl = d.scratch;  // words 0..3: queue head, CTAs done, error bits, timeout flag
+    p.ctl = d.scratch;  // words 0..4: queue head, CTAs done, error bits, timeout flag, continuation count
     p.block_cnt = d.scratch + 8;
     p.block_nodes = d.scratch + 8;  // unused: this variant counts no nodes
     p.sum_out = (unsigned long long *)d_sum;
-    p.nodes_out = d.scratch + 4;
+    p.nodes_out = d.scratch + 5;
     p.status_out = (unsigned long long *)d_sum + 1;
     p.k_one = 1;
     p.k_two = 2;
     p.k_mone = 0xffffffffu;
 
     cudaStream_t s = (cudaStream_t)stream;
-    // The previous call left its control words behind: clear them.
+    // The previous call left its control words behind (queue head, done
+    // ticket, error and timeout words): clear all of them.
     e = cudaMemsetAsync(d.scratch, 0, kCtlWords * sizeof(unsigned long long), s);
     if (e != cudaSuccess) return noalloc_fail(e, "cudaMemsetAsync");
     noalloc_kernel()<<<grid, threads, smem, s>>>(p);

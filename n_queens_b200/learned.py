@@ -57,9 +57,17 @@ def _declare():
     L.nq_schedule_device.restype = ctypes.c_int
     L.nq_schedule_device.argtypes = [_mlpp, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.nq_schedule_device_last.restype = ctypes.c_int
+    L.nq_schedule_device_last.argtypes = [_mlpp, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p]
     L.nq_count_learned.restype = ctypes.c_int
     L.nq_count_learned.argtypes = [ctypes.c_int, ctypes.c_int, _mlpp, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
                                    ctypes.POINTER(Stats)]
+    L.nq_count_learned_reuse.restype = ctypes.c_int
+    L.nq_count_learned_reuse.argtypes = [ctypes.c_int, ctypes.c_int, _mlpp, ctypes.POINTER(ctypes.c_int64),
+                                         ctypes.c_int64, ctypes.c_uint64, ctypes.c_void_p,
+                                         ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(Stats)]
 
 
 _declare()
@@ -169,6 +177,13 @@ class BuildReport:
     holdout_rmse: float = float("nan")
     train_samples: int = 0
     finetune_samples: int = 0
+    # The target board's tasks that the build counted exactly while labelling
+    # (fine-tuning sample and hold-out), and the plain sum of their counts:
+    # count_learned(..., reuse=report) skips them and adds the sum.
+    target_N: int = 0
+    k: int = 0
+    counted_idx: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    counted_sum: int = 0
 
 
 def build_cost_model(target_N: int, k: int = 6, train_N=(16, 17, 18), finetune_frac: float = 0.05,
@@ -201,8 +216,9 @@ def build_cost_model(target_N: int, k: int = 6, train_N=(16, 17, 18), finetune_f
     perm = rng.permutation(cols.size)
     sample = np.sort(perm[:nsample])
     t = time.perf_counter()
-    fc, fl, fr, fy, _, _ = solver_labels(target_N, k, index=sample)
+    fc, fl, fr, fy, _, fcnt = solver_labels(target_N, k, index=sample)
     rep.finetune_label_s = time.perf_counter() - t
+    counted = [(sample, fcnt)]
     rep.finetune_samples = int(nsample)
     t = time.perf_counter()
     rep.finetune_losses = model.train(np.full(nsample, target_N, np.uint8), fc, fl, fr, fy, ft_epochs, batch, lr,
@@ -211,19 +227,39 @@ def build_cost_model(target_N: int, k: int = 6, train_N=(16, 17, 18), finetune_f
     # Hold-out quality on prefixes outside the fine-tuning sample.
     ho = np.sort(perm[nsample:nsample + min(holdout, cols.size - nsample)])
     if ho.size:
-        hc, hl, hr, hy, _, _ = solver_labels(target_N, k, index=ho)
+        hc, hl, hr, hy, _, hcnt = solver_labels(target_N, k, index=ho)
+        counted.append((ho, hcnt))
         pred = model.predict(target_N, hc, hl, hr)
         rep.holdout_spearman = spearman(pred, hy)
         rep.holdout_rmse = float(np.sqrt(np.mean((pred.astype(np.float64) - hy) ** 2)))
+    idx = np.concatenate([i for i, _ in counted]).astype(np.int64)
+    cnt = np.concatenate([c for _, c in counted])
+    o = np.argsort(idx, kind="stable")
+    rep.target_N, rep.k = target_N, k
+    rep.counted_idx = np.ascontiguousarray(idx[o])
+    rep.counted_sum = int(cnt.sum(dtype=np.uint64))
     return model, rep
 
 
-def count_learned(N: int, rows: int, model: CostModel, config=None) -> CountResult:
-    """Whole-board count with the model's longest-first order (nq_count_learned)."""
+def count_learned(N: int, rows: int, model: CostModel, config=None, reuse: BuildReport | None = None) -> CountResult:
+    """Whole-board count with the model's longest-first order (nq_count_learned).
+
+    With ``reuse`` (the report of the build that made ``model`` for this
+    board), the tasks the build already counted exactly are left out of the
+    queue and their sum is added (nq_count_learned_reuse): the labelling work
+    becomes part of the count."""
     tot = ctypes.c_uint64(0)
     st = Stats()
     cfg = _cfg(config)
-    rc = lib.nq_count_learned(N, rows, model._m, ctypes.cast(cfg, ctypes.c_void_p) if cfg else None,
-                              ctypes.byref(tot), ctypes.byref(st))
-    _check(rc, "nq_count_learned")
+    cfgp = ctypes.cast(cfg, ctypes.c_void_p) if cfg else None
+    if reuse is None:
+        rc = lib.nq_count_learned(N, rows, model._m, cfgp, ctypes.byref(tot), ctypes.byref(st))
+        _check(rc, "nq_count_learned")
+    else:
+        if (reuse.target_N, reuse.k) != (N, rows):
+            raise ValueError(f"the report labels N={reuse.target_N} k={reuse.k}, not N={N} k={rows}")
+        idx = np.ascontiguousarray(reuse.counted_idx, np.int64)
+        rc = lib.nq_count_learned_reuse(N, rows, model._m, idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                        idx.size, reuse.counted_sum, cfgp, ctypes.byref(tot), ctypes.byref(st))
+        _check(rc, "nq_count_learned_reuse")
     return CountResult(int(tot.value), None, st.as_dict())

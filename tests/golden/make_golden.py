@@ -1,7 +1,7 @@
 """Generates the golden fixtures in this directory from the reference itself.
 
 Every value here comes from the reference's own code, compiled unchanged from
-its sources into ``oracle/_ref/libnq_ref.so`` (``make -C oracle``): its
+its sources into ``oracle/_ref/libnq_ref.so`` (``make -C oracle REF_SRC=<reference>/src``): its
 expander ``partial_n_queens`` / ``partial_n_queens_for_odd``
 (src/n_queens.cpp:74-113), its recursion ``n_queens`` (src/n_queens.cpp:8-21)
 and its ``serial_n_queens`` (src/n_queens.cpp:115-137).  The published totals
@@ -153,7 +153,7 @@ def main():
     ap.add_argument("--threads", type=int, default=0)
     args = ap.parse_args()
     if not oracle.ref_available():
-        sys.exit("oracle/_ref/libnq_ref.so is not built: run make -C oracle where the reference sources exist")
+        sys.exit("oracle/_ref/libnq_ref.so is not built: run make -C oracle REF_SRC=<reference>/src")
     t = time.time()
     json.dump(gen_expander(), open(os.path.join(HERE, "expander.json"), "w"), indent=1)
     json.dump(gen_totals(), open(os.path.join(HERE, "totals_ref.json"), "w"), indent=1)

@@ -37,6 +37,37 @@ def test_reference_arm_line():
     assert d["config"]["N"] == 16 and d["steps"] == 1 and d["warmup"] == 1
 
 
+def test_reference_arm_loads_no_product_library():
+    # The reference arm must run only the reference's code (oracle/_ref) and
+    # the checkers; the product library may not even be mapped.
+    code = ("import runpy, sys; sys.argv = ['bench.py'] + %r; "
+            "runpy.run_path('bench.py', run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('PRODUCT_MAPPED' if 'libnqueens_b200' in maps else 'PRODUCT_NOT_MAPPED')" % (ARGS,))
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    assert "PRODUCT_NOT_MAPPED" in r.stdout
+    d = _json_lines(r.stdout)[0]
+    if d["cpu_baseline"]["kind"] == "reference":
+        assert "schedule(dynamic,1)" in d["cpu_baseline"]["sample"]
+
+
+def test_reference_log_parser():
+    # The reference CLI's timestamped lines (src/utils.cpp:14-30), its job
+    # lines (src/n_queens_cuda.cu:154,178) and result line (src/main.cpp:53).
+    sys.path.insert(0, ROOT)
+    import bench
+    text = ("[2026-01-02 03:04:05.000] ====\n"
+            "[2026-01-02 03:04:05.080] Use 80.00ms to generate 4470757 subproblems!\n"
+            "[2026-01-02 03:04:06.250] gpu [0] start job, with 4470757(1.000) subproblems.\n"
+            "[2026-01-02 03:04:32.050] gpu [0] finish job.\n"
+            "[2026-01-02 03:04:32.100] cuda 21 queens result 314666222712, calc time: [27100.00ms]\n")
+    starts, finishes, result, calc = bench.parse_reference_log(text)
+    assert result == 314666222712 and calc == 27100.0
+    assert len(starts) == 1 and len(finishes) == 1
+    assert abs((finishes[0] - starts[0]) - 25.8) < 1e-6
+
+
 def test_reference_arm_under_torchrun_two_ranks():
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes", "1", "--nproc-per-node", "2",

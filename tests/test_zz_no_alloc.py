@@ -62,3 +62,70 @@ def test_noalloc_rejects_grid_beyond_its_array(gpu):
                                                torch.cuda.current_stream().cuda_stream)
     assert rc == gpu.NQ_ERR_ARG
     assert "scratch array" in gpu.last_error()
+
+
+def test_noalloc_status_word_does_not_leak_into_the_next_call(gpu):
+    # A call whose tasks need more stack levels than it was given sets the
+    # depth bit (1) of its status word; the next, correct call on the same
+    # shared array must report status 0 and the allocating entry's sum.
+    import torch
+    stream = torch.cuda.current_stream()
+    N, k = 15, 5
+    n, tc, tl, tr = _device_tasks(torch, N, k)
+    bad = gpu.Config()
+    bad.stack_levels = N - 2 - k  # one level short
+    got = torch.full((2,), -7, dtype=torch.int64, device="cuda:0")
+    _run(gpu, gpu.lib.nq_count_tasks_device_noalloc, N, n, tc, tl, tr, got, bad, stream)
+    torch.cuda.synchronize()
+    assert int(got[1]) & 1
+    good = gpu.Config()
+    good.stack_levels = N - 1 - k
+    want = torch.zeros(2, dtype=torch.int64, device="cuda:0")
+    rc = gpu.lib.nq_count_tasks_device(N, tc.data_ptr(), tl.data_ptr(), tr.data_ptr(), n, None, None,
+                                       want.data_ptr(), ctypes.byref(good), stream.cuda_stream)
+    assert rc == 0
+    _run(gpu, gpu.lib.nq_count_tasks_device_noalloc, N, n, tc, tl, tr, got, good, stream)
+    torch.cuda.synchronize()
+    assert int(got[1]) == 0
+    assert got.tolist() == want.tolist()
+    assert 2 * int(got[0]) == oracle.total(N, k)
+
+
+def test_noalloc_runs_the_allocating_entrys_launch_shape(gpu, golden):
+    # Both entries pick the CTA size and queue chunking the same way, so at
+    # the N=19, k=6 whole board they count the same total in about the same
+    # time (kernel time per entry, CUDA events on the launching stream).
+    import torch
+    stream = torch.cuda.current_stream()
+    N, k = 19, 6
+    c, l, r = gpu.expand(N, k)
+    dev = torch.device("cuda:0")
+    tc, tl, tr = (torch.from_numpy(a.view(np.int32)).to(dev) for a in (c, l, r))
+    cfg = gpu.Config()
+    cfg.stack_levels = N - 1 - k
+    outs, ms = {}, {}
+    for name in ("nq_count_tasks_device", "nq_count_tasks_device_noalloc", "nq_count_tasks_device",
+                 "nq_count_tasks_device_noalloc"):
+        fn = getattr(gpu.lib, name)
+        out = torch.full((2,), -7, dtype=torch.int64, device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if name.endswith("noalloc"):
+            rc = fn(N, tc.data_ptr(), tl.data_ptr(), tr.data_ptr(), c.size, out.data_ptr(), ctypes.byref(cfg),
+                    stream.cuda_stream)
+        else:
+            rc = fn(N, tc.data_ptr(), tl.data_ptr(), tr.data_ptr(), c.size, None, None, out.data_ptr(),
+                    ctypes.byref(cfg), stream.cuda_stream)
+        assert rc == 0, gpu.last_error()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        outs.setdefault(name, []).append(out.tolist())
+        ms.setdefault(name, []).append(e0.elapsed_time(e1))
+    want = golden("published.json")[str(N)]["total"]
+    for name, vals in outs.items():
+        for v in vals:
+            assert 2 * v[0] == want and v[1] == 0, (name, v)
+    a, b = min(ms["nq_count_tasks_device"]), min(ms["nq_count_tasks_device_noalloc"])
+    print(f"N={N} k={k}: allocating entry {a:.1f} ms, allocation-free entry {b:.1f} ms")
+    assert b <= 1.05 * a
+
