@@ -63,7 +63,7 @@ enum { NQ_LAYOUT_INTERLEAVED = 0, NQ_LAYOUT_LANE_MAJOR = 1 };
 /* Launch parameters; zero-initialise and set what you need.  Zero means
  * "default" (the autotuned or built-in choice) for every field. */
 typedef struct nq_config {
-    int block_threads;      /* threads per CTA: 32..1024, multiple of 32; 0 = the size (64..1024) that keeps
+    int block_threads;      /* threads per CTA: 32..1024, multiple of 32; 0 = the size (64..512) that keeps
                                the most warps resident per SM for the launch's stack depth */
     int blocks_per_sm;      /* resident CTAs per SM for the persistent grid */
     int stack_levels;       /* per-lane DFS stack slots (>= N-1-rows)  */

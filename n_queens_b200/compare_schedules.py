@@ -3,13 +3,15 @@ expander order, on one GPU (the comparison the cost model exists for).
 
     python -m n_queens_b200.compare_schedules --N 22 --k 6 [--repeats 1] [--json out.json]
                                               [--schedules plain,learned,dihedral]
+                                              [--block-threads 0,192,512]
 
 Builds the cost model once (solver-logged node counts at N=16..18, fine-tuned
 on a seeded 5% sample of the target's prefixes), then alternates plain and
 learned whole-board counts through the public API (nq_count and
 nq_count_learned), each with per-CTA timing, and prints wall time, kernel
 time, makespan, tail-idle fraction and the count of every run.  `dihedral`
-adds the 8-fold decomposition (nq_count_dihedral) to the same alternation.
+adds the 8-fold decomposition (nq_count_dihedral) to the same alternation;
+`--block-threads` alternates CTA sizes inside each schedule.
 """
 from __future__ import annotations
 
@@ -29,7 +31,10 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--json", default=None)
     ap.add_argument("--schedules", default="plain,learned", help="comma list of plain, learned, dihedral")
+    ap.add_argument("--block-threads", default="0",
+                    help="comma list of CTA sizes to alternate (0 = the library's default choice)")
     args = ap.parse_args()
+    threads = [int(x) for x in args.block_threads.split(",") if x]
     names = [x for x in args.schedules.split(",") if x]
     out = {"N": args.N, "k": args.k, "runs": []}
     model = None
@@ -42,20 +47,24 @@ def main():
               flush=True)
     for it in range(args.repeats):
         for name in names:
-            t = time.perf_counter()
-            if name == "plain":
-                r = count(args.N, args.k, config=dict(timing=1))
-            elif name == "dihedral":
-                r = count_dihedral(args.N, args.k, config=dict(timing=1))
-            else:
-                r = learned.count_learned(args.N, args.k, model, config=dict(timing=1))
-            wall = time.perf_counter() - t
-            st = r.stats
-            row = {"schedule": name, "repeat": it, "total": r.total, "wall_s": wall, "kernel_ms": st["kernel_ms"],
-                   "schedule_ms": st["schedule_ms"], "makespan_ms": st["makespan_ms"],
-                   "tail_idle_frac": st["tail_idle_frac"], "expand_ms": st["expand_ms"], "tasks": st["tasks"]}
-            out["runs"].append(row)
-            print(json.dumps(row), flush=True)
+            for bt in threads:
+                cfg = dict(timing=1, block_threads=bt)
+                t = time.perf_counter()
+                if name == "plain":
+                    r = count(args.N, args.k, config=cfg)
+                elif name == "dihedral":
+                    r = count_dihedral(args.N, args.k, config=cfg)
+                else:
+                    r = learned.count_learned(args.N, args.k, model, config=cfg)
+                wall = time.perf_counter() - t
+                st = r.stats
+                row = {"schedule": name, "repeat": it, "total": r.total, "wall_s": wall,
+                       "kernel_ms": st["kernel_ms"], "schedule_ms": st["schedule_ms"],
+                       "makespan_ms": st["makespan_ms"], "tail_idle_frac": st["tail_idle_frac"],
+                       "expand_ms": st["expand_ms"], "tasks": st["tasks"], "block_threads": st["block_threads"],
+                       "grid": st["grid"], "stack_levels": st["stack_levels"]}
+                out["runs"].append(row)
+                print(json.dumps(row), flush=True)
     if args.json:
         with open(args.json, "w") as f:
             json.dump(out, f, indent=1)

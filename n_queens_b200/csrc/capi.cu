@@ -65,10 +65,10 @@ double now_ms() {
 typedef void (*KernelFn)(DfsParams);
 
 KernelFn pick_kernel(bool per_owner, bool nodes, bool dih = false) {
-    if (dih) return per_owner ? dfs_kernel<true, false, 1, kUnroll, false, true>
-                              : dfs_kernel<false, false, 1, kUnroll, false, true>;
-    if (per_owner) return nodes ? dfs_kernel<true, true, 1, kUnroll> : dfs_kernel<true, false, 1, kUnroll>;
-    return nodes ? dfs_kernel<false, true, 1, kUnroll> : dfs_kernel<false, false, 1, kUnroll>;
+    if (dih) return per_owner ? dfs_kernel<true, false, kStepVar, kUnroll, false, true>
+                              : dfs_kernel<false, false, kStepVar, kUnroll, false, true>;
+    if (per_owner) return nodes ? dfs_kernel<true, true, kStepVar, kUnroll> : dfs_kernel<true, false, kStepVar, kUnroll>;
+    return nodes ? dfs_kernel<false, true, kStepVar, kUnroll> : dfs_kernel<false, false, kStepVar, kUnroll>;
 }
 
 struct DevBuf {
@@ -147,9 +147,9 @@ int ensure_ready(Ctx &c, int dev) {
         for (int nd = 0; nd < 2; ++nd)
             NQ_CUDA(cudaFuncSetAttribute(pick_kernel(po, nd), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          c.smem_optin - static_smem));
-    NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, 1, kUnroll, true>,
+    NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, kStepVar, kUnroll, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, c.smem_optin - static_smem));
-    NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, 1, kUnroll, true, true>,
+    NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, kStepVar, kUnroll, true, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, c.smem_optin - static_smem));
     for (int po = 0; po < 2; ++po)
         NQ_CUDA(cudaFuncSetAttribute(pick_kernel(po, false, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -265,6 +265,7 @@ DfsParams base_params(Ctx &c, int N, int64_t n, const nq_config *cfg) {
     p.k_one = 1;
     p.k_two = 2;
     p.k_mone = 0xffffffffu;
+    p.k_half = 0x80000000u;
     p.block_nodes = c.d_ctl + kWordBlocks + (size_t)c.sms * kMaxBlocksPerSm;
     if (cfg && cfg->timing) p.cta_times = c.d_ctl + kWordBlocks + 2 * (size_t)c.sms * kMaxBlocksPerSm;
     return p;
@@ -831,7 +832,7 @@ int count_resumable_impl(int N, int rows, const nq_config *cfg, const char *chec
         NQ_CUDA(cudaMemcpyAsync(d_cont_in, ck.cont.data(), ncont * 16, cudaMemcpyHostToDevice, c.stream));
         if (dih) NQ_CUDA(cudaMemcpyAsync(d_cont_cls, ck.cls.data(), ncont, cudaMemcpyHostToDevice, c.stream));
     }
-    KernelFn fn = dih ? dfs_kernel<false, false, 1, kUnroll, true, true> : dfs_kernel<false, false, 1, kUnroll, true>;
+    KernelFn fn = dih ? dfs_kernel<false, false, kStepVar, kUnroll, true, true> : dfs_kernel<false, false, kStepVar, kUnroll, true>;
     Launch L;
     rc = plan_launch(c, cfg, N - 1 - rows, false, false, L, dih);
     if (rc) return rc;

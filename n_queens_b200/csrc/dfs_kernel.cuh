@@ -77,6 +77,7 @@ struct DfsParams {
     unsigned long long *nodes_out;   // total nodes (device word, NODES)
     unsigned long long *status_out;  // kStat* bits of this launch (device word)
     uint32_t k_one, k_two, k_mone;   // 1, 2, -1 (see dfs_step)
+    uint32_t k_half;                 // 0x80000000: mad.hi by it halves (see dfs_step)
     unsigned long long *cta_times;   // optional [2*gridDim.x]: %globaltimer at CTA start and end
     int layout;                      // stack layout: 0 interleaved (default), 1 lane-major
     // Resumable runs.  Queue positions [0, n_cont_in) are continuation entries
@@ -137,28 +138,15 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
 // parameters, so the compiler cannot fold the multiply-adds below back into
 // ALU adds/moves.
 //
-// VAR 0 issues everything as logic/ALU operations.  VAR 1 moves the adds,
-// the left shift and the four register moves to multiply-add form (the FMA
-// pipe), leaving the LOP3/shift/compare work on the ALU pipe: about 11
-// instructions on each pipe per step instead of ~17 ALU + 7 FMA.
+// VAR 1 issues the adds, the left shift and the four register moves in
+// multiply-add form (the FMA pipe), leaving the LOP3/shift/compare work on the
+// ALU pipe: about 11 instructions on each pipe per step (an all-ALU form ran
+// ~17 ALU + 7 FMA and was 20 % slower).  VAR 2 (below) removes two ALU
+// operations from VAR 1.
 #define NQB_STEP_HEAD                                                                 \
     "{\n\t"                                                                           \
     ".reg .pred pb, pd, pp, pe, pq;\n\t"                                              \
     ".reg .b32 t, bit, nc, nl, nr, na;\n\t"
-
-#define NQB_STEP_CHILD_VAR0                                                           \
-    "neg.s32 t, %3;\n\t"                                                              \
-    "and.b32 bit, t, %3;\n\t"                                                         \
-    "xor.b32 %3, %3, bit;\n\t"                                                        \
-    "or.b32 nc, %0, bit;\n\t"                                                         \
-    "or.b32 nl, %1, bit;\n\t"                                                         \
-    "shl.b32 nl, nl, 1;\n\t"                                                          \
-    "or.b32 nr, %2, bit;\n\t"                                                         \
-    "shr.s32 nr, nr, 1;\n\t"                                                          \
-    "lop3.b32 na, nc, nl, nr, 0x01;\n\t"                                              \
-    "setp.eq.u32 pe, nc, 0xffffffff;\n\t"                                             \
-    "@pe add.u32 %5, %5, 1;\n\t"                                                      \
-    "setp.ne.u32 pb, bit, 0;\n\t"
 
 #define NQB_STEP_CHILD_VAR1                                                           \
     "mul.lo.s32 t, %3, %10;\n\t"                                                      \
@@ -174,23 +162,7 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "setp.eq.u32 pe, nc, 0xffffffff;\n\t"                                             \
     "@pe mad.lo.s32 %5, %8, %8, %5;\n\t"
 
-#define NQB_STEP_NODES_VAR0 "@pb add.u32 %6, %6, 1;\n\t"
 #define NQB_STEP_NODES_VAR1 "@pb mad.lo.s32 %6, %8, %8, %6;\n\t"
-
-#define NQB_STEP_TAIL_VAR0                                                            \
-    "setp.ne.and.u32 pd, na, 0, pb;\n\t"                                              \
-    "setp.ne.and.u32 pp, %3, 0, pd;\n\t"                                              \
-    "@pp st.shared.v4.u32 [%4], {%0, %1, %2, %3};\n\t"                                \
-    "@pp add.u32 %4, %4, %11;\n\t"                                                    \
-    "@pd mov.b32 %0, nc;\n\t"                                                         \
-    "@pd mov.b32 %1, nl;\n\t"                                                         \
-    "@pd mov.b32 %2, nr;\n\t"                                                         \
-    "@pd mov.b32 %3, na;\n\t"                                                         \
-    "setp.eq.u32 pq, %3, 0;\n\t"                                                      \
-    "setp.ne.and.u32 pq, %4, %7, pq;\n\t"                                             \
-    "@pq sub.u32 %4, %4, %11;\n\t"                                                    \
-    "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"                                \
-    "}\n\t"
 
 #define NQB_STEP_TAIL_VAR1                                                            \
     "setp.ne.and.u32 pd, na, 0, pb;\n\t"                                              \
@@ -200,6 +172,44 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "@pd mul.lo.s32 %0, nc, %8;\n\t"                                                  \
     "@pd mul.lo.s32 %1, nl, %8;\n\t"                                                  \
     "@pd mul.lo.s32 %2, nr, %8;\n\t"                                                  \
+    "@pd mul.lo.s32 %3, na, %8;\n\t"                                                  \
+    "setp.eq.u32 pq, %3, 0;\n\t"                                                      \
+    "setp.ne.and.u32 pq, %4, %7, pq;\n\t"                                             \
+    "@pq mad.lo.s32 %4, %10, %11, %4;\n\t"                                            \
+    "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"                                \
+    "}\n\t"
+
+// VAR 2 keeps the two diagonal masks of a level pre-shifted for its
+// children: register ld holds (left << 1) and rd holds (right >> 1, arithmetic),
+// where left/right are the reference's masks of the row being enumerated.  A
+// child's masks are then one multiply-add each,
+//   child left  = ((left | bit) << 1)  = ld + 2*bit            (mad.lo by %9 = 2)
+//   child right = ((right | bit) >> 1) = rd + bit/2            (mad.hi by %12 = 2^31)
+// (bit is free, so it is in neither mask and | equals +), and the shift for
+// the grandchildren is folded into the descend move of each mask.  Two ALU
+// operations fewer per step than VAR 1 (the | and the >> of each diagonal),
+// same stack traffic; the completion count goes to the ALU pipe, leaving 10
+// ALU and 10 FMA-pipe instructions per step.  %12 = 0x80000000.
+#define NQB_STEP_CHILD_VAR2                                                           \
+    "mul.lo.s32 t, %3, %10;\n\t"                                                      \
+    "and.b32 bit, t, %3;\n\t"                                                         \
+    "setp.ne.u32 pb, bit, 0;\n\t"                                                     \
+    "mad.lo.s32 %3, bit, %10, %3;\n\t"                                                \
+    "mad.lo.s32 nc, bit, %8, %0;\n\t"                                                 \
+    "mad.lo.s32 nl, bit, %9, %1;\n\t"                                                 \
+    "mad.hi.u32 nr, bit, %12, %2;\n\t"                                                \
+    "lop3.b32 na, nc, nl, nr, 0x01;\n\t"                                              \
+    "setp.eq.u32 pe, nc, 0xffffffff;\n\t"                                             \
+    "@pe add.u32 %5, %5, 1;\n\t"
+
+#define NQB_STEP_TAIL_VAR2                                                            \
+    "setp.ne.and.u32 pd, na, 0, pb;\n\t"                                              \
+    "setp.ne.and.u32 pp, %3, 0, pd;\n\t"                                              \
+    "@pp st.shared.v4.u32 [%4], {%0, %1, %2, %3};\n\t"                                \
+    "@pp mad.lo.s32 %4, %8, %11, %4;\n\t"                                             \
+    "@pd mul.lo.s32 %0, nc, %8;\n\t"                                                  \
+    "@pd mul.lo.s32 %1, nl, %9;\n\t"                                                  \
+    "@pd shr.s32 %2, nr, 1;\n\t"                                                      \
     "@pd mul.lo.s32 %3, na, %8;\n\t"                                                  \
     "setp.eq.u32 pq, %3, 0;\n\t"                                                      \
     "setp.ne.and.u32 pq, %4, %7, pq;\n\t"                                             \
@@ -241,6 +251,26 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "selp.b32 w, %16, %15, px;\n\t"                                                   \
     "@pe add.u32 %5, %5, w;\n\t"
 
+// The dihedral child of VAR 2 (pre-shifted diagonals, %18 = 0x80000000).
+#define NQB_STEP_CHILD_DIH2                                                           \
+    "mul.lo.s32 t, %3, %10;\n\t"                                                      \
+    "and.b32 bit, t, %3;\n\t"                                                         \
+    "setp.ne.u32 pb, bit, 0;\n\t"                                                     \
+    "mad.lo.s32 %3, bit, %10, %3;\n\t"                                                \
+    "mad.lo.s32 nc, bit, %8, %0;\n\t"                                                 \
+    "mad.lo.s32 nl, bit, %9, %1;\n\t"                                                 \
+    "mad.hi.u32 nr, bit, %18, %2;\n\t"                                                \
+    "lop3.b32 na, nc, nl, nr, 0x01;\n\t"                                              \
+    "popc.b32 pc, nc;\n\t"                                                            \
+    "setp.gt.u32 ps, pc, %12;\n\t"                                                    \
+    "setp.eq.u32 pl, pc, 31;\n\t"                                                     \
+    "selp.b32 msk, %13, %17, pl;\n\t"                                                 \
+    "@ps and.b32 na, na, msk;\n\t"                                                    \
+    "setp.eq.u32 pe, nc, 0xffffffff;\n\t"                                             \
+    "setp.eq.u32 px, bit, %14;\n\t"                                                   \
+    "selp.b32 w, %16, %15, px;\n\t"                                                   \
+    "@pe add.u32 %5, %5, w;\n\t"
+
 // Class registers of a lane in a DIH kernel (cls: the class index, kept for
 // the deadline dump of resumable runs).
 struct DihLane {
@@ -249,20 +279,46 @@ struct DihLane {
 
 struct StepConsts {
     uint32_t one, two, mone, stride;  // stride: bytes between a lane's consecutive stack slots
+    uint32_t half;                    // 0x80000000
 };
+
+// Step variant of every instantiation: 2 = pre-shifted diagonals (default),
+// 1 = the reference's mask form with IMAD-form moves.
+#ifndef NQB_STEP_VAR
+#define NQB_STEP_VAR 2
+#endif
+constexpr int kStepVar = NQB_STEP_VAR;
+static_assert(kStepVar == 1 || kStepVar == 2, "step variant");
+
+// Lane registers (ld, rd) from the reference's (left, right) masks of the row
+// a level enumerates, and back (for the checkpoint file, which stores the
+// reference's form).  Going back loses left's bit 31 and right's bit 0, which
+// no later row can see: a left bit only moves further left, and right's bit
+// 0 falls off the board at the next shift; the level's own free columns are
+// kept separately (its untried mask).
+template <int VAR>
+__device__ __forceinline__ uint32_t lane_ld(uint32_t left) { return VAR == 2 ? left << 1 : left; }
+template <int VAR>
+__device__ __forceinline__ uint32_t lane_rd(uint32_t right) {
+    return VAR == 2 ? (uint32_t)((int32_t)right >> 1) : right;
+}
+template <int VAR>
+__device__ __forceinline__ uint32_t ref_ld(uint32_t ld) { return VAR == 2 ? ld >> 1 : ld; }
+template <int VAR>
+__device__ __forceinline__ uint32_t ref_rd(uint32_t rd) { return VAR == 2 ? rd << 1 : rd; }
 
 template <bool NODES, int VAR>
 __device__ __forceinline__ void dfs_step(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail, uint32_t &sp,
                                          uint32_t &cnt, uint32_t &it, uint32_t bot, const StepConsts &k) {
 #define NQB_STEP_OPERANDS                                                                         \
     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)                   \
-    : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride)                                \
+    : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(k.half)                   \
     : "memory"
-    if (VAR == 0) {
+    if (VAR == 2) {
         if (NODES)
-            asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR0 NQB_STEP_NODES_VAR0 NQB_STEP_TAIL_VAR0 NQB_STEP_OPERANDS);
+            asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR2 NQB_STEP_NODES_VAR1 NQB_STEP_TAIL_VAR2 NQB_STEP_OPERANDS);
         else
-            asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR0 NQB_STEP_TAIL_VAR0 NQB_STEP_OPERANDS);
+            asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR2 NQB_STEP_TAIL_VAR2 NQB_STEP_OPERANDS);
     } else {
         if (NODES)
             asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR1 NQB_STEP_NODES_VAR1 NQB_STEP_TAIL_VAR1 NQB_STEP_OPERANDS);
@@ -272,14 +328,22 @@ __device__ __forceinline__ void dfs_step(uint32_t &cols, uint32_t &ld, uint32_t 
 #undef NQB_STEP_OPERANDS
 }
 
+template <int VAR>
 __device__ __forceinline__ void dfs_step_dih(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail, uint32_t &sp,
                                              uint32_t &cnt, uint32_t &it, uint32_t bot, const StepConsts &k,
                                              const DihLane &d, uint32_t noside) {
-    asm volatile(NQB_STEP_HEAD_DIH NQB_STEP_CHILD_DIH NQB_STEP_TAIL_VAR1
-                 : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
-                 : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(d.side_popc), "r"(d.last_mask),
-                   "r"(d.tie_bit), "r"(d.w), "r"(d.w_tie), "r"(noside)
-                 : "memory");
+    if (VAR == 2)
+        asm volatile(NQB_STEP_HEAD_DIH NQB_STEP_CHILD_DIH2 NQB_STEP_TAIL_VAR2
+                     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
+                     : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(d.side_popc),
+                       "r"(d.last_mask), "r"(d.tie_bit), "r"(d.w), "r"(d.w_tie), "r"(noside), "r"(k.half)
+                     : "memory");
+    else
+        asm volatile(NQB_STEP_HEAD_DIH NQB_STEP_CHILD_DIH NQB_STEP_TAIL_VAR1
+                     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
+                     : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(d.side_popc),
+                       "r"(d.last_mask), "r"(d.tie_bit), "r"(d.w), "r"(d.w_tie), "r"(noside)
+                     : "memory");
 }
 
 __device__ __forceinline__ void load_class_index(const DfsParams &p, uint32_t idx, DihLane &d) {
@@ -300,6 +364,7 @@ __device__ __forceinline__ void load_class(const DfsParams &p, long long t, DihL
 // (1 for an already-complete board) and leaves avail == 0 when the task has
 // no free column.  A column mask with off-board bits can never equal `last`,
 // so such a task counts 0, exactly as the reference recursion does.
+template <int VAR>
 __device__ __forceinline__ uint32_t load_task(const DfsParams &p, long long t, uint32_t &cols, uint32_t &ld,
                                               uint32_t &rd, uint32_t &avail) {
     const int n = p.task_n ? (int)p.task_n[t] : p.N;
@@ -318,8 +383,8 @@ __device__ __forceinline__ uint32_t load_task(const DfsParams &p, long long t, u
         return 0;
     }
     cols = c | ~last;
-    ld = l;
-    rd = r;
+    ld = lane_ld<VAR>(l);
+    rd = lane_rd<VAR>(r);
     avail = ~(cols | l | r);
     return 0;
 }
@@ -348,7 +413,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                                  : smem_base + warp * (uint32_t)p.levels * kSlotBytes + lane * 16u;
 
     if (p.cta_times && threadIdx.x == 0) p.cta_times[2 * blockIdx.x] = globaltimer_ns();
-    const StepConsts kc{p.k_one, p.k_two, p.k_mone, stride};
+    const StepConsts kc{p.k_one, p.k_two, p.k_mone, stride, p.k_half};
     uint32_t cols = 0, ld = 0, rd = 0, avail = 0;
     uint32_t sp = my_base, bot = my_base;
     uint32_t cnt = 0, it = 0;
@@ -418,8 +483,8 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                             atomicOr(p.ctl + kCtlError, kErrDepth);
                         } else {
                             cols = e.x;
-                            ld = e.y;
-                            rd = e.z;
+                            ld = lane_ld<VAR>(e.y);
+                            rd = lane_rd<VAR>(e.z);
                             avail = e.w;
                             // a saved level already carries its class's rules in avail
                             if (DIH) load_class_index(p, p.cont_in_cls[q], dih);
@@ -432,7 +497,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                         // A permutation entry out of range is skipped, never dereferenced.
                         if (t >= 0 && t < p.ntasks) {
                             sp = bot = my_base;
-                            uint32_t done = load_task(p, t, cols, ld, rd, avail);
+                            uint32_t done = load_task<VAR>(p, t, cols, ld, rd, avail);
                             if (DIH) {
                                 load_class(p, t, dih);
                                 done *= dih.w;
@@ -511,7 +576,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
 #pragma unroll
                 for (int u = 0; u < UNROLL; ++u) {
                     if (DIH)
-                        dfs_step_dih(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
+                        dfs_step_dih<VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
                     else
                         dfs_step<NODES, VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
                 }
@@ -522,7 +587,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
 #pragma unroll
                 for (int u = 0; u < UNROLL; ++u) {
                     if (DIH)
-                        dfs_step_dih(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
+                        dfs_step_dih<VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
                     else
                         dfs_step<NODES, VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
                 }
@@ -543,7 +608,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
             atomicOr(p.ctl + kCtlError, kErrContOverflow);
         } else if (mine) {
             if (avail) {
-                p.cont_out[at] = make_uint4(cols, ld, rd, avail);
+                p.cont_out[at] = make_uint4(cols, ref_ld<VAR>(ld), ref_rd<VAR>(rd), avail);
                 if (p.cont_out_owner) p.cont_out_owner[at] = owner;
                 if (DIH) p.cont_out_cls[at] = (uint8_t)dih.cls;
                 ++at;
@@ -551,7 +616,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
             for (uint32_t a = bot; a != sp; a += stride, ++at) {
                 uint32_t x, y, z, w;
                 lds128(a, x, y, z, w);
-                p.cont_out[at] = make_uint4(x, y, z, w);
+                p.cont_out[at] = make_uint4(x, ref_ld<VAR>(y), ref_rd<VAR>(z), w);
                 if (p.cont_out_owner) p.cont_out_owner[at] = owner;
                 if (DIH) p.cont_out_cls[at] = (uint8_t)dih.cls;
             }

@@ -62,7 +62,7 @@ NoAllocDev g_noalloc_dev[kNoAllocMaxDevices];
 
 typedef void (*NoAllocKernel)(DfsParams);
 // The same instantiation the allocating device entry runs for a plain count.
-NoAllocKernel noalloc_kernel() { return dfs_kernel<false, false, 1, kUnroll>; }
+NoAllocKernel noalloc_kernel() { return dfs_kernel<false, false, kStepVar, kUnroll>; }
 
 int noalloc_fail(cudaError_t e, const char *what) {
     set_last_error((std::string(what) + ": " + cudaGetErrorString(e)).c_str());
@@ -221,6 +221,7 @@ extern "C" int nq_count_tasks_device_noalloc(int N, const uint32_t *d_cols, cons
     p.k_one = 1;
     p.k_two = 2;
     p.k_mone = 0xffffffffu;
+    p.k_half = 0x80000000u;
 
     cudaStream_t s = (cudaStream_t)stream;
     // The previous call left its control words behind (queue head, done
