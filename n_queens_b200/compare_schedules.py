@@ -3,7 +3,7 @@ expander order, on one GPU (the comparison the cost model exists for).
 
     python -m n_queens_b200.compare_schedules --N 22 --k 6 [--repeats 1] [--json out.json]
                                               [--schedules plain,learned,dihedral]
-                                              [--block-threads 0,192,512]
+                                              [--block-threads 0,192,512] [--reuse]
 
 Builds the cost model once (solver-logged node counts at N=16..18, fine-tuned
 on a seeded 5% sample of the target's prefixes), then alternates plain and
@@ -11,7 +11,8 @@ learned whole-board counts through the public API (nq_count and
 nq_count_learned), each with per-CTA timing, and prints wall time, kernel
 time, makespan, tail-idle fraction and the count of every run.  `dihedral`
 adds the 8-fold decomposition (nq_count_dihedral) to the same alternation;
-`--block-threads` alternates CTA sizes inside each schedule.
+`--block-threads` alternates CTA sizes inside each schedule; `--reuse` makes
+the learned counts skip the tasks that the model build already counted.
 """
 from __future__ import annotations
 
@@ -33,11 +34,13 @@ def main():
     ap.add_argument("--schedules", default="plain,learned", help="comma list of plain, learned, dihedral")
     ap.add_argument("--block-threads", default="0",
                     help="comma list of CTA sizes to alternate (0 = the library's default choice)")
+    ap.add_argument("--reuse", action="store_true",
+                    help="learned counts skip the tasks the model build counted exactly (nq_count_learned_reuse)")
     args = ap.parse_args()
     threads = [int(x) for x in args.block_threads.split(",") if x]
     names = [x for x in args.schedules.split(",") if x]
     out = {"N": args.N, "k": args.k, "runs": []}
-    model = None
+    model = rep = None
     if "learned" in names:
         t = time.perf_counter()
         model, rep = learned.build_cost_model(args.N, k=args.k, seed=args.seed)
@@ -55,7 +58,7 @@ def main():
                 elif name == "dihedral":
                     r = count_dihedral(args.N, args.k, config=cfg)
                 else:
-                    r = learned.count_learned(args.N, args.k, model, config=cfg)
+                    r = learned.count_learned(args.N, args.k, model, config=cfg, reuse=rep if args.reuse else None)
                 wall = time.perf_counter() - t
                 st = r.stats
                 row = {"schedule": name, "repeat": it, "total": r.total, "wall_s": wall,
