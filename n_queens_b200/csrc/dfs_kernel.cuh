@@ -217,6 +217,108 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"                                \
     "}\n\t"
 
+// VAR 3 is VAR 2 with the predicates taken from LOP3's predicate output
+// (p = (result != 0) op q) instead of separate compares:
+//   lop3.and bit|pb      bit = avail & -avail,  pb = bit != 0
+//   lop3.and na|pd       na = ~(c|l|r),         pd = na != 0 && pb    (descend)
+//   lop3.or  avail|pk    avail ^= bit,          pk = avail != 0 || pd (level goes on)
+//   setp pp = avail != 0 && pd (push),  setp pq = sp != bot && !pk (pop)
+// 19 instructions per step (8 ALU, 9 FMA pipe, 2 shared), against 22.  The
+// steps of one unroll group share one asm block, whose head sets the constant
+// predicate `pt1` (true) once.  Operands as in VAR 2.
+#define NQB_STEP3_HEAD                                                                \
+    "{\n\t"                                                                           \
+    ".reg .pred pt1, pb, pd, pk, pp, pe, pq;\n\t"                                     \
+    ".reg .b32 t, bit, nc, nl, nr, na;\n\t"                                           \
+    "setp.ne.u32 pt1, %8, 0;\n\t"
+
+#define NQB_STEP3_CHILD                                                               \
+    "mul.lo.s32 t, %3, %10;\n\t"                                                      \
+    "lop3.and.b32 bit|pb, t, %3, 0, 0xC0, pt1;\n\t"                                   \
+    "mad.lo.s32 nc, bit, %8, %0;\n\t"                                                 \
+    "mad.lo.s32 nl, bit, %9, %1;\n\t"                                                 \
+    "mad.hi.u32 nr, bit, %12, %2;\n\t"                                                \
+    "lop3.and.b32 na|pd, nc, nl, nr, 0x01, pb;\n\t"                                   \
+    "lop3.or.b32 %3|pk, %3, bit, 0, 0x3C, pd;\n\t"                                    \
+    "setp.eq.u32 pe, nc, 0xffffffff;\n\t"                                             \
+    "@pe add.u32 %5, %5, 1;\n\t"
+
+#define NQB_STEP3_TAIL                                                                \
+    "setp.ne.and.u32 pp, %3, 0, pd;\n\t"                                              \
+    "@pp st.shared.v4.u32 [%4], {%0, %1, %2, %3};\n\t"                                \
+    "@pp mad.lo.s32 %4, %8, %11, %4;\n\t"                                             \
+    "@pd mul.lo.s32 %0, nc, %8;\n\t"                                                  \
+    "@pd mul.lo.s32 %1, nl, %9;\n\t"                                                  \
+    "@pd shr.s32 %2, nr, 1;\n\t"                                                      \
+    "@pd mul.lo.s32 %3, na, %8;\n\t"                                                  \
+    "setp.ne.and.u32 pq, %4, %7, !pk;\n\t"                                            \
+    "@pq mad.lo.s32 %4, %10, %11, %4;\n\t"                                            \
+    "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"
+
+#define NQB_STEP3 NQB_STEP3_CHILD NQB_STEP3_TAIL
+#define NQB_STEP3_NODES NQB_STEP3_CHILD NQB_STEP_NODES_VAR1 NQB_STEP3_TAIL
+#define NQB_STEP3_X4 NQB_STEP3 NQB_STEP3 NQB_STEP3 NQB_STEP3
+#define NQB_STEP3_NODES_X4 NQB_STEP3_NODES NQB_STEP3_NODES NQB_STEP3_NODES NQB_STEP3_NODES
+
+// VAR 4 ("filtered") enumerates only children that have a future.  A child C
+// of the level (placed at column `bit`) lists the columns of the next row it
+// may try (free = ~(c|l|r)); such a column b is dead when the row after it
+// would have no free column at all.  With F0 = the free columns of that row
+// before b is placed (~(c | l<<1 | r>>1), in lane form ~(c | ld | rd)), b is
+// dead exactly when F0 lies inside {b-1, b, b+1}, i.e. when no column of F0 is
+// two or more away from b.  The alive columns are therefore
+//   (columns >= lowest(F0) + 2) | (columns <= highest(F0) - 2)
+//   = -(lo << 2) | (0xffffffff >> (33 - bfind(F0)))          (empty when F0 = 0)
+// and the child's list becomes free & that mask.  A child on row N-2 (its
+// column mask has 30 bits set, off-board bits included) is not entered: every
+// alive column of it completes the board on row N-1, so the step adds the
+// popcount of its filtered list.  Rows N-2 and N-1 are never stepped and dead
+// children never cost a step or a stack push: at N=18, k=6 the steps fall from
+// 29.7e9 to 18.6e9 and the pushes from 7.8e9 to 5.0e9, for 33 instructions per
+// step instead of 19.  Tasks and saved levels on rows N-2 and N-1 are counted
+// when they are loaded.  Operands as in VAR 3 plus %13 = 33, %14 = -4, %15 = 30.
+#define NQB_STEP4_HEAD                                                                \
+    "{\n\t"                                                                           \
+    ".reg .pred pt1, pb, pg, p2, pd, pk, pp, pq;\n\t"                                 \
+    ".reg .b32 t, bit, nc, nl, nr, na, xl, xr, f0, lo, ma, mb, pos, pc, naf;\n\t"     \
+    "setp.ne.u32 pt1, %8, 0;\n\t"
+
+#define NQB_STEP4                                                                     \
+    "mul.lo.s32 t, %3, %10;\n\t"                                                      \
+    "lop3.and.b32 bit|pb, t, %3, 0, 0xC0, pt1;\n\t"                                   \
+    "mad.lo.s32 nc, bit, %8, %0;\n\t"                                                 \
+    "mad.lo.s32 nl, bit, %9, %1;\n\t"                                                 \
+    "mad.hi.u32 nr, bit, %12, %2;\n\t"                                                \
+    "lop3.b32 na, nc, nl, nr, 0x01;\n\t"                                              \
+    "mul.lo.s32 xl, nl, %9;\n\t"                                                      \
+    "shr.s32 xr, nr, 1;\n\t"                                                          \
+    "lop3.b32 f0, nc, xl, xr, 0x01;\n\t"                                              \
+    "mul.lo.s32 t, f0, %10;\n\t"                                                      \
+    "and.b32 lo, t, f0;\n\t"                                                          \
+    "mul.lo.s32 ma, lo, %14;\n\t"                                                     \
+    "bfind.u32 pos, f0;\n\t"                                                          \
+    "mad.lo.s32 pos, pos, %10, %13;\n\t"                                              \
+    "shr.b32 mb, %10, pos;\n\t"                                                       \
+    "popc.b32 pc, nc;\n\t"                                                            \
+    "setp.ne.and.u32 pg, pc, %15, pb;\n\t"                                            \
+    "setp.eq.and.u32 p2, pc, %15, pb;\n\t"                                            \
+    "lop3.and.b32 naf|pd, na, ma, mb, 0xE0, pg;\n\t"                                  \
+    "popc.b32 t, naf;\n\t"                                                            \
+    "@p2 mad.lo.s32 %5, t, %8, %5;\n\t"                                               \
+    "lop3.or.b32 %3|pk, %3, bit, 0, 0x3C, pd;\n\t"                                    \
+    "setp.ne.and.u32 pp, %3, 0, pd;\n\t"                                              \
+    "@pp st.shared.v4.u32 [%4], {%0, %1, %2, %3};\n\t"                                \
+    "@pp mad.lo.s32 %4, %8, %11, %4;\n\t"                                             \
+    "@pd mul.lo.s32 %0, nc, %8;\n\t"                                                  \
+    "@pd mul.lo.s32 %1, xl, %8;\n\t"                                                  \
+    "@pd mul.lo.s32 %2, xr, %8;\n\t"                                                  \
+    "@pd mul.lo.s32 %3, naf, %8;\n\t"                                                 \
+    "setp.ne.and.u32 pq, %4, %7, !pk;\n\t"                                            \
+    "@pq mad.lo.s32 %4, %10, %11, %4;\n\t"                                            \
+    "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"
+
+#define NQB_STEP4_X4 NQB_STEP4 NQB_STEP4 NQB_STEP4 NQB_STEP4
+
 // Dihedral step: the VAR 1 step plus the class rules of the lane's task.
 //   pc = popc(child cols) = 32 - N + child row
 //   pc > %12            -> the child row may not use the side columns, and
@@ -282,13 +384,31 @@ struct StepConsts {
     uint32_t half;                    // 0x80000000
 };
 
-// Step variant of every instantiation: 2 = pre-shifted diagonals (default),
-// 1 = the reference's mask form with IMAD-form moves.
+// Step variant of the count kernels: 4 = filtered children (default), 3 =
+// pre-shifted diagonals with LOP3 predicate outputs, 2 = pre-shifted
+// diagonals, 1 = the reference's mask form with IMAD-form moves.  2, 3 and 4
+// keep the same lane registers.  Kernels that count DFS nodes (NODES) step
+// every placement, so they run variant 3 when 4 is chosen.
 #ifndef NQB_STEP_VAR
-#define NQB_STEP_VAR 2
+#define NQB_STEP_VAR 4
 #endif
 constexpr int kStepVar = NQB_STEP_VAR;
-static_assert(kStepVar == 1 || kStepVar == 2, "step variant");
+static_assert(kStepVar >= 1 && kStepVar <= 4, "step variant");
+constexpr int kNodesStepVar = kStepVar == 4 ? 3 : kStepVar;
+
+// The alive part of level's untried columns (VAR 4): drops every column whose
+// child would leave the next row without a free column.  ld/rd in lane form
+// (pre-shifted), so ~(cols | ld | rd) is that next row's free set before the
+// column is placed.
+__device__ __forceinline__ uint32_t alive_columns(uint32_t cols, uint32_t ld, uint32_t rd, uint32_t avail) {
+    const uint32_t f0 = ~(cols | ld | rd);
+    if (f0 == 0) return 0;
+    const uint32_t lo = f0 & (0u - f0);
+    const int hi = 31 - __clz(f0);
+    const uint32_t above = 0u - (lo << 2);                       // columns >= lowest + 2
+    const uint32_t below = hi >= 2 ? (0xffffffffu >> (33 - hi)) : 0u;  // columns <= highest - 2
+    return avail & (above | below);
+}
 
 // Lane registers (ld, rd) from the reference's (left, right) masks of the row
 // a level enumerates, and back (for the checkpoint file, which stores the
@@ -297,15 +417,15 @@ static_assert(kStepVar == 1 || kStepVar == 2, "step variant");
 // 0 falls off the board at the next shift; the level's own free columns are
 // kept separately (its untried mask).
 template <int VAR>
-__device__ __forceinline__ uint32_t lane_ld(uint32_t left) { return VAR == 2 ? left << 1 : left; }
+__device__ __forceinline__ uint32_t lane_ld(uint32_t left) { return VAR >= 2 ? left << 1 : left; }
 template <int VAR>
 __device__ __forceinline__ uint32_t lane_rd(uint32_t right) {
-    return VAR == 2 ? (uint32_t)((int32_t)right >> 1) : right;
+    return VAR >= 2 ? (uint32_t)((int32_t)right >> 1) : right;
 }
 template <int VAR>
-__device__ __forceinline__ uint32_t ref_ld(uint32_t ld) { return VAR == 2 ? ld >> 1 : ld; }
+__device__ __forceinline__ uint32_t ref_ld(uint32_t ld) { return VAR >= 2 ? ld >> 1 : ld; }
 template <int VAR>
-__device__ __forceinline__ uint32_t ref_rd(uint32_t rd) { return VAR == 2 ? rd << 1 : rd; }
+__device__ __forceinline__ uint32_t ref_rd(uint32_t rd) { return VAR >= 2 ? rd << 1 : rd; }
 
 template <bool NODES, int VAR>
 __device__ __forceinline__ void dfs_step(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail, uint32_t &sp,
@@ -346,6 +466,40 @@ __device__ __forceinline__ void dfs_step_dih(uint32_t &cols, uint32_t &ld, uint3
                      : "memory");
 }
 
+// UNROLL steps of VAR 4 (no NODES form), four per asm block.
+template <int UNROLL>
+__device__ __forceinline__ void dfs_steps4(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail, uint32_t &sp,
+                                           uint32_t &cnt, uint32_t bot, const StepConsts &k) {
+    static_assert(UNROLL % 4 == 0, "VAR 4 unrolls in groups of 4");
+#pragma unroll
+    for (int g = 0; g < UNROLL / 4; ++g)
+        asm volatile(NQB_STEP4_HEAD NQB_STEP4_X4 "}\n\t"
+                     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt)
+                     : "r"(0u), "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(k.half),
+                       "r"(33u), "r"(0xfffffffcu), "r"(30u)
+                     : "memory");
+}
+
+// UNROLL steps of VAR 3 in one asm block (UNROLL a multiple of 4).
+template <bool NODES, int UNROLL>
+__device__ __forceinline__ void dfs_steps3(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail, uint32_t &sp,
+                                           uint32_t &cnt, uint32_t &it, uint32_t bot, const StepConsts &k) {
+    static_assert(UNROLL % 4 == 0, "VAR 3 unrolls in groups of 4");
+#pragma unroll
+    for (int g = 0; g < UNROLL / 4; ++g) {
+        if (NODES)
+            asm volatile(NQB_STEP3_HEAD NQB_STEP3_NODES_X4 "}\n\t"
+                         : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
+                         : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(k.half)
+                         : "memory");
+        else
+            asm volatile(NQB_STEP3_HEAD NQB_STEP3_X4 "}\n\t"
+                         : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
+                         : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(k.half)
+                         : "memory");
+    }
+}
+
 __device__ __forceinline__ void load_class_index(const DfsParams &p, uint32_t idx, DihLane &d) {
     const uint4 c = __ldg(p.cls_tab + idx);
     d.cls = idx;
@@ -358,6 +512,26 @@ __device__ __forceinline__ void load_class_index(const DfsParams &p, uint32_t id
 
 __device__ __forceinline__ void load_class(const DfsParams &p, long long t, DihLane &d) {
     load_class_index(p, __ldg(p.task_cls + t), d);
+}
+
+// VAR 4 keeps only levels on rows 0..N-3, with their alive columns.  A level
+// on row N-1 (one column left) completes once per free column; on row N-2
+// once per alive column.  Returns those completions and leaves avail = 0 for
+// such levels; otherwise filters avail and returns 0.
+__device__ __forceinline__ uint32_t settle_level(int n, uint32_t cols, uint32_t ld, uint32_t rd, uint32_t &avail) {
+    const int row = __popc(cols) - (32 - n);
+    if (row >= n - 1) {
+        const uint32_t done = __popc(avail);
+        avail = 0;
+        return done;
+    }
+    avail = alive_columns(cols, ld, rd, avail);
+    if (row == n - 2) {
+        const uint32_t done = __popc(avail);
+        avail = 0;
+        return done;
+    }
+    return 0;
 }
 
 // Loads task t into a lane.  Returns the completions credited immediately
@@ -386,6 +560,7 @@ __device__ __forceinline__ uint32_t load_task(const DfsParams &p, long long t, u
     ld = lane_ld<VAR>(l);
     rd = lane_rd<VAR>(r);
     avail = ~(cols | l | r);
+    if (VAR == 4) return settle_level(n, cols, ld, rd, avail);
     return 0;
 }
 
@@ -396,6 +571,7 @@ __device__ __forceinline__ uint32_t load_task(const DfsParams &p, long long t, u
 // weights, see DfsParams::cls_tab) and the step is dfs_step_dih.
 template <bool PER_OWNER, bool NODES, int VAR, int UNROLL, bool RESUME = false, bool DIH = false>
 __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
+    static_assert(!(VAR == 4 && (NODES || DIH)), "the filtered step counts no nodes and has no dihedral form");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long red_cnt[32];
     __shared__ unsigned long long red_nodes[32];
@@ -486,6 +662,8 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                             ld = lane_ld<VAR>(e.y);
                             rd = lane_rd<VAR>(e.z);
                             avail = e.w;
+                            // a level saved on row N-2 or N-1 (by a kernel that steps those rows)
+                            if (VAR == 4 && !DIH) tot += settle_level(p.N, cols, ld, rd, avail);
                             // a saved level already carries its class's rules in avail
                             if (DIH) load_class_index(p, p.cont_in_cls[q], dih);
                             if (PER_OWNER && avail) owner = p.cont_in_owner ? p.cont_in_owner[q] : 0u;
@@ -574,9 +752,13 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
         if (check_idle) {
             for (int s = 0; s < p.inner; s += UNROLL) {
 #pragma unroll
-                for (int u = 0; u < UNROLL; ++u) {
+                for (int u = 0; u < (VAR >= 3 && !DIH ? 1 : UNROLL); ++u) {
                     if (DIH)
-                        dfs_step_dih<VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
+                        dfs_step_dih<VAR >= 3 ? 2 : VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
+                    else if (VAR == 4)
+                        dfs_steps4<UNROLL>(cols, ld, rd, avail, sp, cnt, bot, kc);
+                    else if (VAR == 3)
+                        dfs_steps3<NODES, UNROLL>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
                     else
                         dfs_step<NODES, VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
                 }
@@ -585,9 +767,13 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
         } else {
             for (int s = 0; s < p.inner; s += UNROLL) {
 #pragma unroll
-                for (int u = 0; u < UNROLL; ++u) {
+                for (int u = 0; u < (VAR >= 3 && !DIH ? 1 : UNROLL); ++u) {
                     if (DIH)
-                        dfs_step_dih<VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
+                        dfs_step_dih<VAR >= 3 ? 2 : VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
+                    else if (VAR == 4)
+                        dfs_steps4<UNROLL>(cols, ld, rd, avail, sp, cnt, bot, kc);
+                    else if (VAR == 3)
+                        dfs_steps3<NODES, UNROLL>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
                     else
                         dfs_step<NODES, VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
                 }
