@@ -65,8 +65,8 @@ double now_ms() {
 typedef void (*KernelFn)(DfsParams);
 
 KernelFn pick_kernel(bool per_owner, bool nodes, bool dih = false) {
-    if (dih) return per_owner ? dfs_kernel<true, false, kNodesStepVar, kUnroll, false, true>
-                              : dfs_kernel<false, false, kNodesStepVar, kUnroll, false, true>;
+    if (dih) return per_owner ? dfs_kernel<true, false, 1, kUnroll, false, true>
+                              : dfs_kernel<false, false, 1, kUnroll, false, true>;
     if (per_owner)
         return nodes ? dfs_kernel<true, true, kNodesStepVar, kUnroll> : dfs_kernel<true, false, kStepVar, kUnroll>;
     return nodes ? dfs_kernel<false, true, kNodesStepVar, kUnroll> : dfs_kernel<false, false, kStepVar, kUnroll>;
@@ -150,7 +150,7 @@ int ensure_ready(Ctx &c, int dev) {
                                          c.smem_optin - static_smem));
     NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, kStepVar, kUnroll, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, c.smem_optin - static_smem));
-    NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, kNodesStepVar, kUnroll, true, true>,
+    NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, 1, kUnroll, true, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, c.smem_optin - static_smem));
     for (int po = 0; po < 2; ++po)
         NQ_CUDA(cudaFuncSetAttribute(pick_kernel(po, false, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -266,7 +266,6 @@ DfsParams base_params(Ctx &c, int N, int64_t n, const nq_config *cfg) {
     p.k_one = 1;
     p.k_two = 2;
     p.k_mone = 0xffffffffu;
-    p.k_half = 0x80000000u;
     p.block_nodes = c.d_ctl + kWordBlocks + (size_t)c.sms * kMaxBlocksPerSm;
     if (cfg && cfg->timing) p.cta_times = c.d_ctl + kWordBlocks + 2 * (size_t)c.sms * kMaxBlocksPerSm;
     return p;
@@ -833,7 +832,7 @@ int count_resumable_impl(int N, int rows, const nq_config *cfg, const char *chec
         NQ_CUDA(cudaMemcpyAsync(d_cont_in, ck.cont.data(), ncont * 16, cudaMemcpyHostToDevice, c.stream));
         if (dih) NQ_CUDA(cudaMemcpyAsync(d_cont_cls, ck.cls.data(), ncont, cudaMemcpyHostToDevice, c.stream));
     }
-    KernelFn fn = dih ? dfs_kernel<false, false, kNodesStepVar, kUnroll, true, true> : dfs_kernel<false, false, kStepVar, kUnroll, true>;
+    KernelFn fn = dih ? dfs_kernel<false, false, 1, kUnroll, true, true> : dfs_kernel<false, false, kStepVar, kUnroll, true>;
     Launch L;
     rc = plan_launch(c, cfg, N - 1 - rows, false, false, L, dih);
     if (rc) return rc;

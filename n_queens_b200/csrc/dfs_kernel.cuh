@@ -77,7 +77,6 @@ struct DfsParams {
     unsigned long long *nodes_out;   // total nodes (device word, NODES)
     unsigned long long *status_out;  // kStat* bits of this launch (device word)
     uint32_t k_one, k_two, k_mone;   // 1, 2, -1 (see dfs_step)
-    uint32_t k_half;                 // 0x80000000: mad.hi by it halves (see dfs_step)
     unsigned long long *cta_times;   // optional [2*gridDim.x]: %globaltimer at CTA start and end
     int layout;                      // stack layout: 0 interleaved (default), 1 lane-major
     // Resumable runs.  Queue positions [0, n_cont_in) are continuation entries
@@ -141,8 +140,7 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
 // VAR 1 issues the adds, the left shift and the four register moves in
 // multiply-add form (the FMA pipe), leaving the LOP3/shift/compare work on the
 // ALU pipe: about 11 instructions on each pipe per step (an all-ALU form ran
-// ~17 ALU + 7 FMA and was 20 % slower).  VAR 2 (below) removes two ALU
-// operations from VAR 1.
+// ~17 ALU + 7 FMA and was 20 % slower).
 #define NQB_STEP_HEAD                                                                 \
     "{\n\t"                                                                           \
     ".reg .pred pb, pd, pp, pe, pq;\n\t"                                              \
@@ -179,53 +177,22 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"                                \
     "}\n\t"
 
-// VAR 2 keeps the two diagonal masks of a level pre-shifted for its
-// children: register ld holds (left << 1) and rd holds (right >> 1, arithmetic),
-// where left/right are the reference's masks of the row being enumerated.  A
-// child's masks are then one multiply-add each,
-//   child left  = ((left | bit) << 1)  = ld + 2*bit            (mad.lo by %9 = 2)
-//   child right = ((right | bit) >> 1) = rd + bit/2            (mad.hi by %12 = 2^31)
-// (bit is free, so it is in neither mask and | equals +), and the shift for
-// the grandchildren is folded into the descend move of each mask.  Two ALU
-// operations fewer per step than VAR 1 (the | and the >> of each diagonal),
-// same stack traffic; the completion count goes to the ALU pipe, leaving 10
-// ALU and 10 FMA-pipe instructions per step.  %12 = 0x80000000.
-#define NQB_STEP_CHILD_VAR2                                                           \
-    "mul.lo.s32 t, %3, %10;\n\t"                                                      \
-    "and.b32 bit, t, %3;\n\t"                                                         \
-    "setp.ne.u32 pb, bit, 0;\n\t"                                                     \
-    "mad.lo.s32 %3, bit, %10, %3;\n\t"                                                \
-    "mad.lo.s32 nc, bit, %8, %0;\n\t"                                                 \
-    "mad.lo.s32 nl, bit, %9, %1;\n\t"                                                 \
-    "mad.hi.u32 nr, bit, %12, %2;\n\t"                                                \
-    "lop3.b32 na, nc, nl, nr, 0x01;\n\t"                                              \
-    "setp.eq.u32 pe, nc, 0xffffffff;\n\t"                                             \
-    "@pe add.u32 %5, %5, 1;\n\t"
-
-#define NQB_STEP_TAIL_VAR2                                                            \
-    "setp.ne.and.u32 pd, na, 0, pb;\n\t"                                              \
-    "setp.ne.and.u32 pp, %3, 0, pd;\n\t"                                              \
-    "@pp st.shared.v4.u32 [%4], {%0, %1, %2, %3};\n\t"                                \
-    "@pp mad.lo.s32 %4, %8, %11, %4;\n\t"                                             \
-    "@pd mul.lo.s32 %0, nc, %8;\n\t"                                                  \
-    "@pd mul.lo.s32 %1, nl, %9;\n\t"                                                  \
-    "@pd shr.s32 %2, nr, 1;\n\t"                                                      \
-    "@pd mul.lo.s32 %3, na, %8;\n\t"                                                  \
-    "setp.eq.u32 pq, %3, 0;\n\t"                                                      \
-    "setp.ne.and.u32 pq, %4, %7, pq;\n\t"                                             \
-    "@pq mad.lo.s32 %4, %10, %11, %4;\n\t"                                            \
-    "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"                                \
-    "}\n\t"
-
-// VAR 3 is VAR 2 with the predicates taken from LOP3's predicate output
-// (p = (result != 0) op q) instead of separate compares:
+// VAR 3 keeps a level's left-diagonal mask pre-shifted for its children
+// (register ld holds left << 1), so a child's left mask is one multiply-add,
+// (left | bit) << 1 = ld + 2*bit (bit is free, so | equals +), and the shift
+// for the grandchildren rides on the descend move (x 2 instead of x 1).  The
+// right diagonal stays in the reference's form: a right shift has no
+// multiply-add form, and a multiply-high in its place loaded the FMA pipe
+// more than the two ALU operations it saved (measured 5-7 % slower).  The
+// predicates come from LOP3's predicate output (p = (result != 0) op q)
+// instead of separate compares:
 //   lop3.and bit|pb      bit = avail & -avail,  pb = bit != 0
 //   lop3.and na|pd       na = ~(c|l|r),         pd = na != 0 && pb    (descend)
 //   lop3.or  avail|pk    avail ^= bit,          pk = avail != 0 || pd (level goes on)
 //   setp pp = avail != 0 && pd (push),  setp pq = sp != bot && !pk (pop)
-// 19 instructions per step (8 ALU, 9 FMA pipe, 2 shared), against 22.  The
-// steps of one unroll group share one asm block, whose head sets the constant
-// predicate `pt1` (true) once.  Operands as in VAR 2.
+// 20 instructions per step (9 ALU, 9 FMA pipe, 2 shared) against VAR 1's 24,
+// same stack traffic.  Four steps share one asm block, whose head sets the
+// constant predicate `pt1` (true) once.  Operands as in VAR 1.
 #define NQB_STEP3_HEAD                                                                \
     "{\n\t"                                                                           \
     ".reg .pred pt1, pb, pd, pk, pp, pe, pq;\n\t"                                     \
@@ -237,7 +204,8 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "lop3.and.b32 bit|pb, t, %3, 0, 0xC0, pt1;\n\t"                                   \
     "mad.lo.s32 nc, bit, %8, %0;\n\t"                                                 \
     "mad.lo.s32 nl, bit, %9, %1;\n\t"                                                 \
-    "mad.hi.u32 nr, bit, %12, %2;\n\t"                                                \
+    "or.b32 nr, %2, bit;\n\t"                                                         \
+    "shr.s32 nr, nr, 1;\n\t"                                                          \
     "lop3.and.b32 na|pd, nc, nl, nr, 0x01, pb;\n\t"                                   \
     "lop3.or.b32 %3|pk, %3, bit, 0, 0x3C, pd;\n\t"                                    \
     "setp.eq.u32 pe, nc, 0xffffffff;\n\t"                                             \
@@ -249,7 +217,7 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "@pp mad.lo.s32 %4, %8, %11, %4;\n\t"                                             \
     "@pd mul.lo.s32 %0, nc, %8;\n\t"                                                  \
     "@pd mul.lo.s32 %1, nl, %9;\n\t"                                                  \
-    "@pd shr.s32 %2, nr, 1;\n\t"                                                      \
+    "@pd mul.lo.s32 %2, nr, %8;\n\t"                                                  \
     "@pd mul.lo.s32 %3, na, %8;\n\t"                                                  \
     "setp.ne.and.u32 pq, %4, %7, !pk;\n\t"                                            \
     "@pq mad.lo.s32 %4, %10, %11, %4;\n\t"                                            \
@@ -264,9 +232,9 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
 // of the level (placed at column `bit`) lists the columns of the next row it
 // may try (free = ~(c|l|r)); such a column b is dead when the row after it
 // would have no free column at all.  With F0 = the free columns of that row
-// before b is placed (~(c | l<<1 | r>>1), in lane form ~(c | ld | rd)), b is
-// dead exactly when F0 lies inside {b-1, b, b+1}, i.e. when no column of F0 is
-// two or more away from b.  The alive columns are therefore
+// before b is placed (~(c | l<<1 | r>>1)), b is dead exactly when F0 lies
+// inside {b-1, b, b+1}, i.e. when no column of F0 is two or more away from
+// b.  The alive columns are therefore
 //   (columns >= lowest(F0) + 2) | (columns <= highest(F0) - 2)
 //   = -(lo << 2) | (0xffffffff >> (33 - bfind(F0)))          (empty when F0 = 0)
 // and the child's list becomes free & that mask.  A child on row N-2 (its
@@ -274,9 +242,10 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
 // alive column of it completes the board on row N-1, so the step adds the
 // popcount of its filtered list.  Rows N-2 and N-1 are never stepped and dead
 // children never cost a step or a stack push: at N=18, k=6 the steps fall from
-// 29.7e9 to 18.6e9 and the pushes from 7.8e9 to 5.0e9, for 33 instructions per
-// step instead of 19.  Tasks and saved levels on rows N-2 and N-1 are counted
-// when they are loaded.  Operands as in VAR 3 plus %13 = 33, %14 = -4, %15 = 30.
+// 29.7e9 to 18.6e9 and the pushes from 7.8e9 to 5.0e9, for 32 instructions per
+// step instead of 20.  Tasks and saved levels on rows N-2 and N-1 are counted
+// when they are loaded.  Lane registers as in VAR 3.  Operands as in VAR 1
+// plus %12 = 33, %13 = -4, %14 = 30.
 #define NQB_STEP4_HEAD                                                                \
     "{\n\t"                                                                           \
     ".reg .pred pt1, pb, pg, p2, pd, pk, pp, pq;\n\t"                                 \
@@ -288,20 +257,21 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "lop3.and.b32 bit|pb, t, %3, 0, 0xC0, pt1;\n\t"                                   \
     "mad.lo.s32 nc, bit, %8, %0;\n\t"                                                 \
     "mad.lo.s32 nl, bit, %9, %1;\n\t"                                                 \
-    "mad.hi.u32 nr, bit, %12, %2;\n\t"                                                \
+    "or.b32 nr, %2, bit;\n\t"                                                         \
+    "shr.s32 nr, nr, 1;\n\t"                                                          \
     "lop3.b32 na, nc, nl, nr, 0x01;\n\t"                                              \
     "mul.lo.s32 xl, nl, %9;\n\t"                                                      \
     "shr.s32 xr, nr, 1;\n\t"                                                          \
     "lop3.b32 f0, nc, xl, xr, 0x01;\n\t"                                              \
     "mul.lo.s32 t, f0, %10;\n\t"                                                      \
     "and.b32 lo, t, f0;\n\t"                                                          \
-    "mul.lo.s32 ma, lo, %14;\n\t"                                                     \
+    "mul.lo.s32 ma, lo, %13;\n\t"                                                     \
     "bfind.u32 pos, f0;\n\t"                                                          \
-    "mad.lo.s32 pos, pos, %10, %13;\n\t"                                              \
+    "mad.lo.s32 pos, pos, %10, %12;\n\t"                                              \
     "shr.b32 mb, %10, pos;\n\t"                                                       \
     "popc.b32 pc, nc;\n\t"                                                            \
-    "setp.ne.and.u32 pg, pc, %15, pb;\n\t"                                            \
-    "setp.eq.and.u32 p2, pc, %15, pb;\n\t"                                            \
+    "setp.ne.and.u32 pg, pc, %14, pb;\n\t"                                            \
+    "setp.eq.and.u32 p2, pc, %14, pb;\n\t"                                            \
     "lop3.and.b32 naf|pd, na, ma, mb, 0xE0, pg;\n\t"                                  \
     "popc.b32 t, naf;\n\t"                                                            \
     "@p2 mad.lo.s32 %5, t, %8, %5;\n\t"                                               \
@@ -311,7 +281,7 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "@pp mad.lo.s32 %4, %8, %11, %4;\n\t"                                             \
     "@pd mul.lo.s32 %0, nc, %8;\n\t"                                                  \
     "@pd mul.lo.s32 %1, xl, %8;\n\t"                                                  \
-    "@pd mul.lo.s32 %2, xr, %8;\n\t"                                                  \
+    "@pd mul.lo.s32 %2, nr, %8;\n\t"                                                  \
     "@pd mul.lo.s32 %3, naf, %8;\n\t"                                                 \
     "setp.ne.and.u32 pq, %4, %7, !pk;\n\t"                                            \
     "@pq mad.lo.s32 %4, %10, %11, %4;\n\t"                                            \
@@ -353,26 +323,6 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "selp.b32 w, %16, %15, px;\n\t"                                                   \
     "@pe add.u32 %5, %5, w;\n\t"
 
-// The dihedral child of VAR 2 (pre-shifted diagonals, %18 = 0x80000000).
-#define NQB_STEP_CHILD_DIH2                                                           \
-    "mul.lo.s32 t, %3, %10;\n\t"                                                      \
-    "and.b32 bit, t, %3;\n\t"                                                         \
-    "setp.ne.u32 pb, bit, 0;\n\t"                                                     \
-    "mad.lo.s32 %3, bit, %10, %3;\n\t"                                                \
-    "mad.lo.s32 nc, bit, %8, %0;\n\t"                                                 \
-    "mad.lo.s32 nl, bit, %9, %1;\n\t"                                                 \
-    "mad.hi.u32 nr, bit, %18, %2;\n\t"                                                \
-    "lop3.b32 na, nc, nl, nr, 0x01;\n\t"                                              \
-    "popc.b32 pc, nc;\n\t"                                                            \
-    "setp.gt.u32 ps, pc, %12;\n\t"                                                    \
-    "setp.eq.u32 pl, pc, 31;\n\t"                                                     \
-    "selp.b32 msk, %13, %17, pl;\n\t"                                                 \
-    "@ps and.b32 na, na, msk;\n\t"                                                    \
-    "setp.eq.u32 pe, nc, 0xffffffff;\n\t"                                             \
-    "setp.eq.u32 px, bit, %14;\n\t"                                                   \
-    "selp.b32 w, %16, %15, px;\n\t"                                                   \
-    "@pe add.u32 %5, %5, w;\n\t"
-
 // Class registers of a lane in a DIH kernel (cls: the class index, kept for
 // the deadline dump of resumable runs).
 struct DihLane {
@@ -381,106 +331,69 @@ struct DihLane {
 
 struct StepConsts {
     uint32_t one, two, mone, stride;  // stride: bytes between a lane's consecutive stack slots
-    uint32_t half;                    // 0x80000000
 };
 
 // Step variant of the count kernels: 4 = filtered children (default), 3 =
-// pre-shifted diagonals with LOP3 predicate outputs, 2 = pre-shifted
-// diagonals, 1 = the reference's mask form with IMAD-form moves.  2, 3 and 4
-// keep the same lane registers.  Kernels that count DFS nodes (NODES) step
-// every placement, so they run variant 3 when 4 is chosen.
+// pre-shifted left diagonal with LOP3 predicate outputs, 1 = the reference's
+// mask form with IMAD-form moves.  Kernels that count DFS nodes (NODES) step
+// every placement, so they run variant 3 when 4 is chosen; the dihedral
+// kernels run variant 1.
 #ifndef NQB_STEP_VAR
 #define NQB_STEP_VAR 4
 #endif
 constexpr int kStepVar = NQB_STEP_VAR;
-static_assert(kStepVar >= 1 && kStepVar <= 4, "step variant");
+static_assert(kStepVar == 1 || kStepVar == 3 || kStepVar == 4, "step variant");
 constexpr int kNodesStepVar = kStepVar == 4 ? 3 : kStepVar;
 
-// The alive part of level's untried columns (VAR 4): drops every column whose
-// child would leave the next row without a free column.  ld/rd in lane form
-// (pre-shifted), so ~(cols | ld | rd) is that next row's free set before the
-// column is placed.
+// Lane registers (ld, rd) from the reference's (left, right) masks of the row
+// a level enumerates, and back (for the checkpoint file, which stores the
+// reference's form).  Going back loses left's bit 31, which no later row can
+// see (a left bit only moves further left).
+template <int VAR>
+__device__ __forceinline__ uint32_t lane_ld(uint32_t left) { return VAR >= 3 ? left << 1 : left; }
+template <int VAR>
+__device__ __forceinline__ uint32_t ref_ld(uint32_t ld) { return VAR >= 3 ? ld >> 1 : ld; }
+
+// The alive part of a level's untried columns (VAR 4): drops every column
+// whose child would leave the next row without a free column.  ld in lane
+// form (pre-shifted), rd in the reference's form.
 __device__ __forceinline__ uint32_t alive_columns(uint32_t cols, uint32_t ld, uint32_t rd, uint32_t avail) {
-    const uint32_t f0 = ~(cols | ld | rd);
+    const uint32_t f0 = ~(cols | ld | (uint32_t)((int32_t)rd >> 1));
     if (f0 == 0) return 0;
     const uint32_t lo = f0 & (0u - f0);
     const int hi = 31 - __clz(f0);
-    const uint32_t above = 0u - (lo << 2);                       // columns >= lowest + 2
+    const uint32_t above = 0u - (lo << 2);                              // columns >= lowest + 2
     const uint32_t below = hi >= 2 ? (0xffffffffu >> (33 - hi)) : 0u;  // columns <= highest - 2
     return avail & (above | below);
 }
 
-// Lane registers (ld, rd) from the reference's (left, right) masks of the row
-// a level enumerates, and back (for the checkpoint file, which stores the
-// reference's form).  Going back loses left's bit 31 and right's bit 0, which
-// no later row can see: a left bit only moves further left, and right's bit
-// 0 falls off the board at the next shift; the level's own free columns are
-// kept separately (its untried mask).
-template <int VAR>
-__device__ __forceinline__ uint32_t lane_ld(uint32_t left) { return VAR >= 2 ? left << 1 : left; }
-template <int VAR>
-__device__ __forceinline__ uint32_t lane_rd(uint32_t right) {
-    return VAR >= 2 ? (uint32_t)((int32_t)right >> 1) : right;
-}
-template <int VAR>
-__device__ __forceinline__ uint32_t ref_ld(uint32_t ld) { return VAR >= 2 ? ld >> 1 : ld; }
-template <int VAR>
-__device__ __forceinline__ uint32_t ref_rd(uint32_t rd) { return VAR >= 2 ? rd << 1 : rd; }
-
 template <bool NODES, int VAR>
 __device__ __forceinline__ void dfs_step(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail, uint32_t &sp,
                                          uint32_t &cnt, uint32_t &it, uint32_t bot, const StepConsts &k) {
-#define NQB_STEP_OPERANDS                                                                         \
-    : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)                   \
-    : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(k.half)                   \
-    : "memory"
-    if (VAR == 2) {
-        if (NODES)
-            asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR2 NQB_STEP_NODES_VAR1 NQB_STEP_TAIL_VAR2 NQB_STEP_OPERANDS);
-        else
-            asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR2 NQB_STEP_TAIL_VAR2 NQB_STEP_OPERANDS);
-    } else {
-        if (NODES)
-            asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR1 NQB_STEP_NODES_VAR1 NQB_STEP_TAIL_VAR1 NQB_STEP_OPERANDS);
-        else
-            asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR1 NQB_STEP_TAIL_VAR1 NQB_STEP_OPERANDS);
-    }
-#undef NQB_STEP_OPERANDS
+    static_assert(VAR == 1, "VAR 3 and 4 run in groups (dfs_steps3, dfs_steps4)");
+    if (NODES)
+        asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR1 NQB_STEP_NODES_VAR1 NQB_STEP_TAIL_VAR1
+                     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
+                     : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride)
+                     : "memory");
+    else
+        asm volatile(NQB_STEP_HEAD NQB_STEP_CHILD_VAR1 NQB_STEP_TAIL_VAR1
+                     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
+                     : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride)
+                     : "memory");
 }
 
-template <int VAR>
 __device__ __forceinline__ void dfs_step_dih(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail, uint32_t &sp,
                                              uint32_t &cnt, uint32_t &it, uint32_t bot, const StepConsts &k,
                                              const DihLane &d, uint32_t noside) {
-    if (VAR == 2)
-        asm volatile(NQB_STEP_HEAD_DIH NQB_STEP_CHILD_DIH2 NQB_STEP_TAIL_VAR2
-                     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
-                     : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(d.side_popc),
-                       "r"(d.last_mask), "r"(d.tie_bit), "r"(d.w), "r"(d.w_tie), "r"(noside), "r"(k.half)
-                     : "memory");
-    else
-        asm volatile(NQB_STEP_HEAD_DIH NQB_STEP_CHILD_DIH NQB_STEP_TAIL_VAR1
-                     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
-                     : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(d.side_popc),
-                       "r"(d.last_mask), "r"(d.tie_bit), "r"(d.w), "r"(d.w_tie), "r"(noside)
-                     : "memory");
+    asm volatile(NQB_STEP_HEAD_DIH NQB_STEP_CHILD_DIH NQB_STEP_TAIL_VAR1
+                 : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
+                 : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(d.side_popc), "r"(d.last_mask),
+                   "r"(d.tie_bit), "r"(d.w), "r"(d.w_tie), "r"(noside)
+                 : "memory");
 }
 
-// UNROLL steps of VAR 4 (no NODES form), four per asm block.
-template <int UNROLL>
-__device__ __forceinline__ void dfs_steps4(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail, uint32_t &sp,
-                                           uint32_t &cnt, uint32_t bot, const StepConsts &k) {
-    static_assert(UNROLL % 4 == 0, "VAR 4 unrolls in groups of 4");
-#pragma unroll
-    for (int g = 0; g < UNROLL / 4; ++g)
-        asm volatile(NQB_STEP4_HEAD NQB_STEP4_X4 "}\n\t"
-                     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt)
-                     : "r"(0u), "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(k.half),
-                       "r"(33u), "r"(0xfffffffcu), "r"(30u)
-                     : "memory");
-}
-
-// UNROLL steps of VAR 3 in one asm block (UNROLL a multiple of 4).
+// UNROLL steps of VAR 3 (UNROLL a multiple of 4), four per asm block.
 template <bool NODES, int UNROLL>
 __device__ __forceinline__ void dfs_steps3(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail, uint32_t &sp,
                                            uint32_t &cnt, uint32_t &it, uint32_t bot, const StepConsts &k) {
@@ -490,14 +403,29 @@ __device__ __forceinline__ void dfs_steps3(uint32_t &cols, uint32_t &ld, uint32_
         if (NODES)
             asm volatile(NQB_STEP3_HEAD NQB_STEP3_NODES_X4 "}\n\t"
                          : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
-                         : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(k.half)
+                         : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride)
                          : "memory");
         else
             asm volatile(NQB_STEP3_HEAD NQB_STEP3_X4 "}\n\t"
                          : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
-                         : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(k.half)
+                         : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride)
                          : "memory");
     }
+}
+
+// UNROLL steps of VAR 4 (no NODES form), four per asm block.  Operand %6 is
+// unused (it stands where the node counter sits in the other forms).
+template <int UNROLL>
+__device__ __forceinline__ void dfs_steps4(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail, uint32_t &sp,
+                                           uint32_t &cnt, uint32_t bot, const StepConsts &k) {
+    static_assert(UNROLL % 4 == 0, "VAR 4 unrolls in groups of 4");
+#pragma unroll
+    for (int g = 0; g < UNROLL / 4; ++g)
+        asm volatile(NQB_STEP4_HEAD NQB_STEP4_X4 "}\n\t"
+                     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt)
+                     : "r"(0u), "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(33u),
+                       "r"(0xfffffffcu), "r"(30u)
+                     : "memory");
 }
 
 __device__ __forceinline__ void load_class_index(const DfsParams &p, uint32_t idx, DihLane &d) {
@@ -558,7 +486,7 @@ __device__ __forceinline__ uint32_t load_task(const DfsParams &p, long long t, u
     }
     cols = c | ~last;
     ld = lane_ld<VAR>(l);
-    rd = lane_rd<VAR>(r);
+    rd = r;
     avail = ~(cols | l | r);
     if (VAR == 4) return settle_level(n, cols, ld, rd, avail);
     return 0;
@@ -572,6 +500,7 @@ __device__ __forceinline__ uint32_t load_task(const DfsParams &p, long long t, u
 template <bool PER_OWNER, bool NODES, int VAR, int UNROLL, bool RESUME = false, bool DIH = false>
 __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
     static_assert(!(VAR == 4 && (NODES || DIH)), "the filtered step counts no nodes and has no dihedral form");
+    static_assert(!(DIH && VAR != 1), "the dihedral step is written for the reference's mask form");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long red_cnt[32];
     __shared__ unsigned long long red_nodes[32];
@@ -589,7 +518,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                                  : smem_base + warp * (uint32_t)p.levels * kSlotBytes + lane * 16u;
 
     if (p.cta_times && threadIdx.x == 0) p.cta_times[2 * blockIdx.x] = globaltimer_ns();
-    const StepConsts kc{p.k_one, p.k_two, p.k_mone, stride, p.k_half};
+    const StepConsts kc{p.k_one, p.k_two, p.k_mone, stride};
     uint32_t cols = 0, ld = 0, rd = 0, avail = 0;
     uint32_t sp = my_base, bot = my_base;
     uint32_t cnt = 0, it = 0;
@@ -660,7 +589,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                         } else {
                             cols = e.x;
                             ld = lane_ld<VAR>(e.y);
-                            rd = lane_rd<VAR>(e.z);
+                            rd = e.z;
                             avail = e.w;
                             // a level saved on row N-2 or N-1 (by a kernel that steps those rows)
                             if (VAR == 4 && !DIH) tot += settle_level(p.N, cols, ld, rd, avail);
@@ -752,12 +681,12 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
         if (check_idle) {
             for (int s = 0; s < p.inner; s += UNROLL) {
 #pragma unroll
-                for (int u = 0; u < (VAR >= 3 && !DIH ? 1 : UNROLL); ++u) {
-                    if (DIH)
-                        dfs_step_dih<VAR >= 3 ? 2 : VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
-                    else if (VAR == 4)
+                for (int u = 0; u < (VAR >= 3 ? 1 : UNROLL); ++u) {
+                    if constexpr (DIH)
+                        dfs_step_dih(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
+                    else if constexpr (VAR == 4)
                         dfs_steps4<UNROLL>(cols, ld, rd, avail, sp, cnt, bot, kc);
-                    else if (VAR == 3)
+                    else if constexpr (VAR == 3)
                         dfs_steps3<NODES, UNROLL>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
                     else
                         dfs_step<NODES, VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
@@ -767,12 +696,12 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
         } else {
             for (int s = 0; s < p.inner; s += UNROLL) {
 #pragma unroll
-                for (int u = 0; u < (VAR >= 3 && !DIH ? 1 : UNROLL); ++u) {
-                    if (DIH)
-                        dfs_step_dih<VAR >= 3 ? 2 : VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
-                    else if (VAR == 4)
+                for (int u = 0; u < (VAR >= 3 ? 1 : UNROLL); ++u) {
+                    if constexpr (DIH)
+                        dfs_step_dih(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
+                    else if constexpr (VAR == 4)
                         dfs_steps4<UNROLL>(cols, ld, rd, avail, sp, cnt, bot, kc);
-                    else if (VAR == 3)
+                    else if constexpr (VAR == 3)
                         dfs_steps3<NODES, UNROLL>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
                     else
                         dfs_step<NODES, VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc);
@@ -794,7 +723,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
             atomicOr(p.ctl + kCtlError, kErrContOverflow);
         } else if (mine) {
             if (avail) {
-                p.cont_out[at] = make_uint4(cols, ref_ld<VAR>(ld), ref_rd<VAR>(rd), avail);
+                p.cont_out[at] = make_uint4(cols, ref_ld<VAR>(ld), rd, avail);
                 if (p.cont_out_owner) p.cont_out_owner[at] = owner;
                 if (DIH) p.cont_out_cls[at] = (uint8_t)dih.cls;
                 ++at;
@@ -802,7 +731,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
             for (uint32_t a = bot; a != sp; a += stride, ++at) {
                 uint32_t x, y, z, w;
                 lds128(a, x, y, z, w);
-                p.cont_out[at] = make_uint4(x, ref_ld<VAR>(y), ref_rd<VAR>(z), w);
+                p.cont_out[at] = make_uint4(x, ref_ld<VAR>(y), z, w);
                 if (p.cont_out_owner) p.cont_out_owner[at] = owner;
                 if (DIH) p.cont_out_cls[at] = (uint8_t)dih.cls;
             }
