@@ -55,8 +55,8 @@ I_ALG = 22  # algorithmic warp-issue slots per DFS node (fixed cost model)
 METRIC = "DFS nodes/s (exact whole-board count, 1 B200)"
 
 # Whole-board workloads: published totals (README.md:16-25, logs/5090.log) and
-# DFS node totals (placements into rows k..N-2, counted by the kernel's node
-# statistics and, up to N=17, by the CPU oracle).
+# DFS node totals (placements into rows k..N-2, counted by the node-counting
+# kernel -- nq_count(..., nodes) -- and, up to N=17, by the CPU oracle).
 WORKLOADS = {
     "n16k5": dict(N=16, k=5, total=14772512, nodes=563126914),
     "n17k6": dict(N=17, k=6, total=95815104, nodes=3959755915),
@@ -64,7 +64,7 @@ WORKLOADS = {
     "n19k6": dict(N=19, k=6, total=4968057848, nodes=228483606026),
     "n20k6": dict(N=20, k=6, total=39029188884, nodes=1865470950135),
     "n21k6": dict(N=21, k=6, total=314666222712, nodes=15916200586353),
-    "n22k6": dict(N=22, k=6, total=2691008701644, nodes=None),
+    "n22k6": dict(N=22, k=6, total=2691008701644, nodes=141911885610183),
 }
 
 
@@ -648,6 +648,11 @@ def run_ours(args, world, rank, local):
     }
     if clocks.get("sm_mhz"):
         roof["frac_at_sampled_clock"] = achieved / (sms * 4 * clocks["sm_mhz"] * 1e6 / 1e9)
+    if n22 is not None:
+        for arm in ("learned", "plain"):
+            r22 = n22[arm]
+            if "nodes_per_s_kernel" in r22:
+                r22["roofline_frac"] = r22["nodes_per_s_kernel"] * I_ALG / 32 / 1e9 / peak
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
