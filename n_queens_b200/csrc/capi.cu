@@ -266,8 +266,6 @@ DfsParams base_params(Ctx &c, int N, int64_t n, const nq_config *cfg) {
     p.k_one = 1;
     p.k_two = 2;
     p.k_mone = 0xffffffffu;
-    p.k_33 = 33u;
-    p.k_m4 = 0xfffffffcu;
     p.block_nodes = c.d_ctl + kWordBlocks + (size_t)c.sms * kMaxBlocksPerSm;
     if (cfg && cfg->timing) p.cta_times = c.d_ctl + kWordBlocks + 2 * (size_t)c.sms * kMaxBlocksPerSm;
     return p;

@@ -77,7 +77,6 @@ struct DfsParams {
     unsigned long long *nodes_out;   // total nodes (device word, NODES)
     unsigned long long *status_out;  // kStat* bits of this launch (device word)
     uint32_t k_one, k_two, k_mone;   // 1, 2, -1 (see dfs_step)
-    uint32_t k_33, k_m4;             // 33, -4 (the filtered step, VAR 4)
     unsigned long long *cta_times;   // optional [2*gridDim.x]: %globaltimer at CTA start and end
     int layout;                      // stack layout: 0 interleaved (default), 1 lane-major
     // Resumable runs.  Queue positions [0, n_cont_in) are continuation entries
@@ -193,13 +192,12 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
 //   setp pp = avail != 0 && pd (push),  setp pq = sp != bot && !pk (pop)
 // 20 instructions per step (9 ALU, 9 FMA pipe, 2 shared) against VAR 1's 24,
 // same stack traffic.  Four steps share one asm block, whose head sets the
-// constant predicate `pt1` (true, a compare of two immediates that ptxas
-// folds).  Operands as in VAR 1.
+// constant predicate `pt1` (true) once.  Operands as in VAR 1.
 #define NQB_STEP3_HEAD                                                                \
     "{\n\t"                                                                           \
     ".reg .pred pt1, pb, pd, pk, pp, pe, pq;\n\t"                                     \
     ".reg .b32 t, bit, nc, nl, nr, na;\n\t"                                           \
-    "setp.eq.u32 pt1, 0, 0;\n\t"
+    "setp.ne.u32 pt1, %8, 0;\n\t"
 
 #define NQB_STEP3_CHILD                                                               \
     "mul.lo.s32 t, %3, %10;\n\t"                                                      \
@@ -247,13 +245,12 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
 // 29.7e9 to 18.6e9 and the pushes from 7.8e9 to 5.0e9, for 32 instructions per
 // step instead of 20.  Tasks and saved levels on rows N-2 and N-1 are counted
 // when they are loaded.  Lane registers as in VAR 3.  Operands as in VAR 1
-// plus %12 = 33, %13 = -4 (both kernel parameters), %14 = 30; `pt1` is the
-// constant-true predicate (a compare of two immediates, which ptxas folds).
+// plus %12 = 33, %13 = -4, %14 = 30.
 #define NQB_STEP4_HEAD                                                                \
     "{\n\t"                                                                           \
     ".reg .pred pt1, pb, pg, p2, pd, pk, pp, pq;\n\t"                                 \
     ".reg .b32 t, bit, nc, nl, nr, na, xl, xr, f0, lo, ma, mb, pos, pc, naf;\n\t"     \
-    "setp.eq.u32 pt1, 0, 0;\n\t"
+    "setp.ne.u32 pt1, %8, 0;\n\t"
 
 #define NQB_STEP4                                                                     \
     "mul.lo.s32 t, %3, %10;\n\t"                                                      \
@@ -334,7 +331,6 @@ struct DihLane {
 
 struct StepConsts {
     uint32_t one, two, mone, stride;  // stride: bytes between a lane's consecutive stack slots
-    uint32_t c33, cm4;                // 33 and -4 (VAR 4), from kernel parameters like the others
 };
 
 // Step variant of the count kernels: 4 = filtered children (default), 3 =
@@ -427,8 +423,8 @@ __device__ __forceinline__ void dfs_steps4(uint32_t &cols, uint32_t &ld, uint32_
     for (int g = 0; g < UNROLL / 4; ++g)
         asm volatile(NQB_STEP4_HEAD NQB_STEP4_X4 "}\n\t"
                      : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt)
-                     : "r"(0u), "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(k.c33),
-                       "r"(k.cm4), "r"(30u)
+                     : "r"(0u), "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(33u),
+                       "r"(0xfffffffcu), "r"(30u)
                      : "memory");
 }
 
@@ -522,7 +518,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                                  : smem_base + warp * (uint32_t)p.levels * kSlotBytes + lane * 16u;
 
     if (p.cta_times && threadIdx.x == 0) p.cta_times[2 * blockIdx.x] = globaltimer_ns();
-    const StepConsts kc{p.k_one, p.k_two, p.k_mone, stride, p.k_33, p.k_m4};
+    const StepConsts kc{p.k_one, p.k_two, p.k_mone, stride};
     uint32_t cols = 0, ld = 0, rd = 0, avail = 0;
     uint32_t sp = my_base, bot = my_base;
     uint32_t cnt = 0, it = 0;

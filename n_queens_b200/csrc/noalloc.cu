@@ -221,8 +221,6 @@ extern "C" int nq_count_tasks_device_noalloc(int N, const uint32_t *d_cols, cons
     p.k_one = 1;
     p.k_two = 2;
     p.k_mone = 0xffffffffu;
-    p.k_33 = 33u;
-    p.k_m4 = 0xfffffffcu;
 
     cudaStream_t s = (cudaStream_t)stream;
     // The previous call left its control words behind (queue head, done
