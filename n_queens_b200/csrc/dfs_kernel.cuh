@@ -8,13 +8,18 @@
 //    (cols, ld, rd, avail); only levels that still have untried columns are
 //    pushed to the lane's shared-memory stack, so a pop always resumes a level
 //    with work and every DFS step places exactly one queen.
+//  * The count kernels' step (VAR 4) lists only a level's alive columns --
+//    those whose child still has a free column in the next row -- and counts
+//    the completions of a row N-2 level from its alive columns instead of
+//    stepping rows N-2 and N-1 (37 % fewer steps at N=18).
 //  * cols carries the off-board bits (~last) pre-set.  Then the free mask is
 //    one LOP3 (~(cols|ld|rd)) with no `& last`, a completed board is
 //    cols == 0xffffffff, and no depth counter is kept at all.
 //  * Stack layout: slot s of lane l in warp w is the 16-byte entry at
 //    w*levels*512 + s*512 + l*16.  Every stack access is a 128-bit LDS/STS and
-//    a quarter-warp always covers 128 contiguous bytes whatever the per-lane
-//    depths are, so no access has a bank conflict (the reference mixes in a
+//    the eight lanes of a quarter-warp always cover the 32 banks once,
+//    whatever the per-lane depths are, so no access needs more wavefronts
+//    than a dense 16-byte access of the warp (the reference mixes in a
 //    32-bit store, src/n_queens_cuda.cu:47, which is 4-way conflicted).
 //  * Tasks come from a device queue: one atomicAdd per warp refill hands a
 //    block of consecutive queue positions to the idle lanes (the reference
