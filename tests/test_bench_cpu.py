@@ -103,3 +103,19 @@ def test_max_over_ranks_gloo():
         p.join(timeout=60)
         assert p.exitcode == 0
     assert res == {0: 2.5, 1: 2.5}
+
+
+def test_reference_cpu_solver_timing_script():
+    # oracle.time_reference_cpu times the reference's own parallel_n_queens
+    # (oracle/_ref); where the reference was not built it says so and exits.
+    sys.path.insert(0, ROOT)
+    import oracle
+    r = subprocess.run([sys.executable, "-m", "oracle.time_reference_cpu", "--N", "12", "--k", "4"], cwd=ROOT,
+                       capture_output=True, text=True, timeout=300)
+    if not oracle.ref_available():
+        assert r.returncode != 0 and "not built" in (r.stderr + r.stdout)
+        return
+    assert r.returncode == 0, r.stderr
+    d = _json_lines(r.stdout)[0]
+    assert d["solver"] == "parallel_n_queens" and d["total"] == 14200 and d["total_ok"]
+    assert d["omp_threads"] == 32 and d["host_cores"] >= 1 and d["seconds"] >= 0
