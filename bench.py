@@ -380,7 +380,7 @@ def run_ours(args, world, rank, local):
     tc = torch.from_numpy(cols.view(np.int32)).to(dev)
     tl = torch.from_numpy(ld.view(np.int32)).to(dev)
     tr = torch.from_numpy(rd.view(np.int32)).to(dev)
-    levels = N - 1 - k
+    levels = nq.stack_levels(N, k)  # stack slots per lane of the count kernel for k-row prefixes
     cfg = nq.Config()
     cfg.device = local
     cfg.stack_levels = levels

@@ -66,7 +66,7 @@ typedef struct nq_config {
     int block_threads;      /* threads per CTA: 32..1024, multiple of 32; 0 = the size (64..512) that keeps
                                the most warps resident per SM for the launch's stack depth */
     int blocks_per_sm;      /* resident CTAs per SM for the persistent grid */
-    int stack_levels;       /* per-lane DFS stack slots (>= N-1-rows)  */
+    int stack_levels;       /* per-lane DFS stack slots (>= nq_stack_levels(N, rows, nodes)) */
     int steal;              /* 0 = default (on), 1 = on, -1 = off: in-warp work donation */
     int inner_steps;        /* DFS steps between warp refill checks (multiple of 4) */
     int order_kind;         /* NQ_ORDER_PLAIN or NQ_ORDER_GIVEN */
@@ -123,6 +123,12 @@ const char *nq_status_string(int status);
 const char *nq_last_error(void);
 /* Number of CUDA devices (0 when none); returns NQ_OK or NQ_ERR_CUDA. */
 int nq_device_count(int *count);
+/* Stack slots per lane (nq_config.stack_levels) that tasks with `rows`
+ * queens placed need: N-1-rows when the count also reports DFS nodes
+ * (nodes != 0), N-3-rows otherwise (the count step never enters rows N-2 and
+ * N-1), at least 1.  The reference fixes this depth at compile time
+ * (STACKSIZE, src/macro.h:25-35).  Returns NQ_ERR_ARG for an invalid (N, rows). */
+int nq_stack_levels(int N, int rows, int nodes);
 
 /* Host prefix expander.  Replaces partial_n_queens + partial_n_queens_for_odd
  * (src/n_queens.cpp:74-113) as cuda_n_queens calls them

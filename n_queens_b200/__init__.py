@@ -141,6 +141,8 @@ def _load() -> ctypes.CDLL:
     L.nq_last_error.restype = ctypes.c_char_p
     L.nq_device_count.restype = ctypes.c_int
     L.nq_device_count.argtypes = [ctypes.POINTER(ctypes.c_int)]
+    L.nq_stack_levels.restype = ctypes.c_int
+    L.nq_stack_levels.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.nq_expand.restype = ctypes.c_int
     L.nq_expand.argtypes = [ctypes.c_int, ctypes.c_int, _u32p, _u32p, _u32p, ctypes.c_int64, _i64p, ctypes.c_int]
     L.nq_expand_device.restype = ctypes.c_int
@@ -191,7 +193,7 @@ def _load() -> ctypes.CDLL:
 lib = _load()
 
 # Every symbol the C header declares (checked by the CPU test suite).
-EXPORTS = ("nq_abi_version", "nq_status_string", "nq_last_error", "nq_device_count", "nq_expand",
+EXPORTS = ("nq_abi_version", "nq_status_string", "nq_last_error", "nq_device_count", "nq_stack_levels", "nq_expand",
            "nq_expand_device", "nq_count",
            "nq_count_resumable",
            "nq_count_tasks", "nq_count_tasks_device", "nq_count_tasks_device_noalloc", "nq_count_batch",
@@ -229,6 +231,14 @@ def _cfg(config) -> ctypes.POINTER(Config) | None:
 
 def _p(a, t):
     return a.ctypes.data_as(t) if a is not None else None
+
+
+def stack_levels(N: int, rows: int, nodes: bool = False) -> int:
+    """Stack slots per lane that a count of (N, rows) prefixes needs (nq_stack_levels)."""
+    v = lib.nq_stack_levels(N, rows, 1 if nodes else 0)
+    if v < 0:
+        raise NQError(v, "nq_stack_levels")
+    return v
 
 
 def device_count() -> int:

@@ -296,13 +296,13 @@ int status_from_bits(unsigned long long bits) {
     return NQ_OK;
 }
 
-int levels_for_tasks(int N, const uint32_t *cols, int64_t n) {
+int levels_for_tasks(int N, const uint32_t *cols, int64_t n, bool filtered) {
     const uint32_t last = (N >= 32) ? 0xffffffffu : ((1u << N) - 1u);
     int need = 1;
     for (int64_t i = 0; i < n; ++i) {
         const uint32_t c = cols[i];
         if ((c & ~last) || c == last) continue;
-        need = std::max(need, N - 1 - __builtin_popcount(c));
+        need = std::max(need, stack_need(N, __builtin_popcount(c), filtered));
     }
     return need;
 }
@@ -694,7 +694,8 @@ int build_batch(Ctx &c, const nq_instance *inst, int64_t n, int split, const nq_
         for (size_t k = before; k < tc.size(); ++k) {
             own.push_back((uint32_t)(2 * u + (tw[k] == 2 ? 1 : 0)));
             tn.push_back((uint8_t)b.N);
-            if (!(tc[k] & ~last) && tc[k] != last) need = std::max(need, b.N - 1 - __builtin_popcount(tc[k]));
+            if (!(tc[k] & ~last) && tc[k] != last)
+                need = std::max(need, stack_need(b.N, __builtin_popcount(tc[k]), true));
         }
     }
     const int64_t m = (int64_t)tc.size();
@@ -834,7 +835,7 @@ int count_resumable_impl(int N, int rows, const nq_config *cfg, const char *chec
     }
     KernelFn fn = dih ? dfs_kernel<false, false, 1, kUnroll, true, true> : dfs_kernel<false, false, kStepVar, kUnroll, true>;
     Launch L;
-    rc = plan_launch(c, cfg, N - 1 - rows, false, false, L, dih);
+    rc = plan_launch(c, cfg, stack_need(N, rows, !dih), false, false, L, dih);
     if (rc) return rc;
     {
         // the resumable instantiation may fit fewer CTAs per SM
@@ -955,6 +956,11 @@ const char *nq_status_string(int status) {
 
 const char *nq_last_error(void) { return g_last_error.c_str(); }
 
+int nq_stack_levels(int N, int rows, int nodes) {
+    if (N < 1 || N > NQ_MAX_N || rows < 0 || rows > N) return NQ_ERR_ARG;
+    return stack_need(N, rows, nodes == 0);
+}
+
 int nq_device_count(int *count) {
     if (!count) return NQ_ERR_ARG;
     int n = 0;
@@ -1074,7 +1080,8 @@ int nq_count(int N, int rows, const nq_config *cfg, uint64_t *total, uint64_t *n
     }
     uint32_t *d = (uint32_t *)c.tasks.p;
     uint64_t sum = 0, nd = 0;
-    rc = count_resident(c, N, d, d + n, d + 2 * n, n, N - 1 - rows, cfg, false, nodes != nullptr, nullptr, nullptr,
+    rc = count_resident(c, N, d, d + n, d + 2 * n, n, stack_need(N, rows, nodes == nullptr), cfg, false,
+                        nodes != nullptr, nullptr, nullptr,
                         &sum, &nd, stats, true);
     // The reference doubles every per-prefix sum for the mirror image
     // (src/n_queens_cuda.cu:181-183).
@@ -1177,7 +1184,7 @@ int count_learned_impl(int N, int rows, nq_mlp *m, const int64_t *done_idx, int6
     }
     NQ_CUDA(cudaEventRecord(e_sched1, c.stream));
     uint64_t sum = 0;
-    rc = count_resident(c, N, d, d + n, d + 2 * n, n, N - 1 - rows, cfg, false, false, nullptr, nullptr, &sum,
+    rc = count_resident(c, N, d, d + n, d + 2 * n, n, stack_need(N, rows, true), cfg, false, false, nullptr, nullptr, &sum,
                         nullptr, stats, true, d_order, nullptr, n - n_done);
     if (stats) {
         float ms = 0;
@@ -1230,7 +1237,7 @@ int nq_count_tasks(int N, const uint32_t *cols, const uint32_t *ld, const uint32
         if (stats) stats->total_ms = now_ms() - t0;
         return NQ_OK;
     }
-    const int need = levels_for_tasks(N, cols, n);
+    const int need = levels_for_tasks(N, cols, n, nodes_per_task == nullptr);
     rc = c.tasks.grow((size_t)n * 12);
     if (rc) return rc;
     uint32_t *d = (uint32_t *)c.tasks.p;
@@ -1269,9 +1276,9 @@ int nq_count_tasks_device(int N, const uint32_t *d_cols, const uint32_t *d_ld, c
     cudaStream_t s = (cudaStream_t)stream;
     // Without a host view of the tasks the stack must cover the deepest
     // possible task (an empty board) unless the caller states the depth.
-    const int need = (cfg && cfg->stack_levels > 0) ? cfg->stack_levels : N - 1;
     const bool per_owner = d_per_task != nullptr;
     const bool want_nodes = d_nodes != nullptr;
+    const int need = (cfg && cfg->stack_levels > 0) ? cfg->stack_levels : stack_need(N, 0, !want_nodes);
     Launch L;
     rc = plan_launch(c, cfg, need, per_owner, want_nodes, L);
     if (rc) return rc;
@@ -1463,7 +1470,7 @@ int nq_count_dihedral(int N, int rows, const nq_config *cfg, uint64_t *total, nq
     NQ_CUDA(cudaEventRecord(c.ev[0], c.stream));
     if (n) NQ_CUDA(cudaMemcpyAsync(d, h, (size_t)n * 13, cudaMemcpyHostToDevice, c.stream));
     uint64_t sum = 0;
-    rc = count_resident(c, N, d, d + n, d + 2 * n, n, N - 1 - rows, cfg, false, false, nullptr, nullptr, &sum,
+    rc = count_resident(c, N, d, d + n, d + 2 * n, n, stack_need(N, rows, false), cfg, false, false, nullptr, nullptr, &sum,
                         nullptr, stats, true, nullptr, &a);
     *total = sum;  // the class weights already carry every symmetry factor
     if (stats) stats->total_ms = now_ms() - t0;
@@ -1501,7 +1508,7 @@ int nq_count_dihedral_tasks(int N, int rows, const uint32_t *cols, const uint32_
     NQ_CUDA(cudaMemcpyAsync(d + n, ld, (size_t)n * 4, cudaMemcpyHostToDevice, c.stream));
     NQ_CUDA(cudaMemcpyAsync(d + 2 * n, rd, (size_t)n * 4, cudaMemcpyHostToDevice, c.stream));
     NQ_CUDA(cudaMemcpyAsync(d + 3 * n, cls, (size_t)n, cudaMemcpyHostToDevice, c.stream));
-    const int need = levels_for_tasks(N, cols, n);
+    const int need = levels_for_tasks(N, cols, n, false);
     rc = count_resident(c, N, d, d + n, d + 2 * n, n, need, cfg, per_task != nullptr, false, per_task, nullptr, sum,
                         nullptr, stats, true, nullptr, &a);
     if (stats) stats->total_ms = now_ms() - t0;

@@ -350,6 +350,12 @@ constexpr int kStepVar = NQB_STEP_VAR;
 static_assert(kStepVar == 1 || kStepVar == 3 || kStepVar == 4, "step variant");
 constexpr int kNodesStepVar = kStepVar == 4 ? 3 : kStepVar;
 
+// Stack rows a step variant never pushes beyond the reference's N-1-rows: the
+// filtered step enters no level on row N-2 or N-1, so the deepest level it
+// pushes is on row N-4.
+template <int VAR>
+constexpr int kStackRowsSpared = VAR == 4 ? 2 : 0;
+
 // Lane registers (ld, rd) from the reference's (left, right) masks of the row
 // a level enumerates, and back (for the checkpoint file, which stores the
 // reference's form).  Going back loses left's bit 31, which no later row can
@@ -483,8 +489,9 @@ __device__ __forceinline__ uint32_t load_task(const DfsParams &p, long long t, u
     if (c & ~last) return 0;
     if (c == last) return 1;
     // Stack slots this task can use: one per level that still has a sibling,
-    // at most N-1-popc(cols).
-    const int need = n - 1 - __popc(c);
+    // at most N-1-popc(cols) -- N-3-popc(cols) for the filtered step, which
+    // never enters rows N-2 and N-1.
+    const int need = n - 1 - __popc(c) - kStackRowsSpared<VAR>;
     if (need > p.levels) {
         atomicOr(p.ctl + kCtlError, kErrDepth);
         return 0;
@@ -588,7 +595,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                         // a level saved by an earlier, interrupted run
                         sp = bot = my_base;
                         const uint4 e = p.cont_in[q];
-                        const int need = __popc(~e.x) - 1;
+                        const int need = __popc(~e.x) - 1 - kStackRowsSpared<VAR>;
                         if (need > p.levels) {
                             atomicOr(p.ctl + kCtlError, kErrDepth);
                         } else {

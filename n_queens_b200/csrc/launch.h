@@ -33,6 +33,14 @@ constexpr int kDfsStaticSmem = 2 * 32 * 8 + 16;
 constexpr int kMinAutoThreads = 64;
 constexpr int kMaxAutoThreads = 512;
 
+// Stack slots per lane that a launch over prefixes with `placed` queens needs:
+// N-1-placed for the kernels that step every row (node counts, the dihedral
+// decomposition), two fewer for the filtered count step.  At least 1.
+inline int stack_need(int N, int placed, bool filtered) {
+    const int need = N - 1 - placed - (filtered && kStepVar == 4 ? kStackRowsSpared<4> : 0);
+    return need < 1 ? 1 : need;
+}
+
 // The CTA size (a multiple of 32 in [64, 512]) that keeps the most warps
 // resident per SM for `levels` stack slots per lane, the larger CTA on a tie;
 // at most cap_per_sm CTAs per SM are counted.  Returns 0 when no size fits.

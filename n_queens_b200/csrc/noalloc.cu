@@ -166,7 +166,7 @@ extern "C" int nq_count_tasks_device_noalloc(int N, const uint32_t *d_cols, cons
     // CTA size that keeps the most warps resident for the stack depth, 1024
     // DFS steps between queue visits), with the grid bounded by the array's
     // per-CTA partials.
-    const int levels = (cfg && cfg->stack_levels > 0) ? cfg->stack_levels : std::max(1, N - 1);
+    const int levels = (cfg && cfg->stack_levels > 0) ? cfg->stack_levels : stack_need(N, 0, true);
     int cap_per_sm = std::min(kNoAllocMaxBlocksPerSm, std::max(1, kNoAllocMaxCtas / d.sms));
     if (cfg && cfg->blocks_per_sm > 0) cap_per_sm = std::min(cap_per_sm, cfg->blocks_per_sm);
     const int threads = (cfg && cfg->block_threads)

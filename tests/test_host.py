@@ -163,3 +163,13 @@ def test_resumable_rejects_foreign_or_broken_checkpoints(tmp_path):
     p.write_bytes(hdr + b"z")                                 # trailing bytes
     assert nq.lib.nq_count_resumable(10, 3, None, str(p).encode(), ctypes.byref(t), ctypes.byref(d), None) \
         == nq.NQ_ERR_ARG
+
+
+def test_stack_levels_of_the_count_kernels():
+    # The count step never enters rows N-2 and N-1, so it needs two stack slots
+    # fewer than the node-counting step (which steps every row, like the
+    # reference's loop with its STACKSIZE, src/macro.h:25-35); at least 1.
+    assert nq.stack_levels(21, 6) == 12 and nq.stack_levels(21, 6, nodes=True) == 14
+    assert nq.stack_levels(16, 5) == 8 and nq.stack_levels(4, 3) == 1
+    with pytest.raises(nq.NQError):
+        nq.stack_levels(40, 6)
