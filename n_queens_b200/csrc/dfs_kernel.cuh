@@ -328,6 +328,62 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "selp.b32 w, %16, %15, px;\n\t"                                                   \
     "@pe add.u32 %5, %5, w;\n\t"
 
+// The dihedral step in the filtered form (the dihedral kernels' default when
+// the count kernels run VAR 4): the left diagonal pre-shifted as in VAR 3, and
+// each child's list cut to its alive columns (those whose next row keeps a free
+// column, ignoring the class rules -- the rules only remove columns, so this
+// drops dead children only) except on row N-1, whose columns complete the
+// board.  Rows N-2 and N-1 are still stepped, because the class rules and the
+// tie weight decide what their completions count.  Operands as in the
+// dihedral step above.
+#define NQB_STEP_HEAD_DIH4                                                            \
+    "{\n\t"                                                                           \
+    ".reg .pred pb, pd, pp, pe, pq, pq0, ps, pl, px;\n\t"                              \
+    ".reg .b32 t, bit, nc, nl, nr, na, pc, msk, w, xl, xr, f0, lo, ma, mb, pos;\n\t"  \
+
+#define NQB_STEP_DIH4                                                                 \
+    "mul.lo.s32 t, %3, %10;\n\t"                                                      \
+    "and.b32 bit, t, %3;\n\t"                                                         \
+    "setp.ne.u32 pb, bit, 0;\n\t"                                                     \
+    "mad.lo.s32 %3, bit, %10, %3;\n\t"                                                \
+    "mad.lo.s32 nc, bit, %8, %0;\n\t"                                                 \
+    "mad.lo.s32 nl, bit, %9, %1;\n\t"                                                 \
+    "or.b32 nr, %2, bit;\n\t"                                                         \
+    "shr.s32 nr, nr, 1;\n\t"                                                          \
+    "lop3.b32 na, nc, nl, nr, 0x01;\n\t"                                              \
+    "popc.b32 pc, nc;\n\t"                                                            \
+    "setp.gt.u32 ps, pc, %12;\n\t"                                                    \
+    "setp.eq.u32 pl, pc, 31;\n\t"                                                     \
+    "selp.b32 msk, %13, %17, pl;\n\t"                                                 \
+    "@ps and.b32 na, na, msk;\n\t"                                                    \
+    "mul.lo.s32 xl, nl, %9;\n\t"                                                      \
+    "shr.s32 xr, nr, 1;\n\t"                                                          \
+    "lop3.b32 f0, nc, xl, xr, 0x01;\n\t"                                              \
+    "mul.lo.s32 t, f0, %10;\n\t"                                                      \
+    "and.b32 lo, t, f0;\n\t"                                                          \
+    "mul.lo.s32 ma, lo, -4;\n\t"                                                      \
+    "bfind.u32 pos, f0;\n\t"                                                          \
+    "mad.lo.s32 pos, pos, %10, 33;\n\t"                                               \
+    "shr.b32 mb, %10, pos;\n\t"                                                       \
+    "@!pl lop3.b32 na, na, ma, mb, 0xE0;\n\t"                                         \
+    "setp.ne.and.u32 pd, na, 0, pb;\n\t"                                              \
+    "setp.eq.u32 pe, nc, 0xffffffff;\n\t"                                             \
+    "setp.eq.u32 px, bit, %14;\n\t"                                                   \
+    "selp.b32 w, %16, %15, px;\n\t"                                                   \
+    "@pe mad.lo.s32 %5, w, %8, %5;\n\t"                                               \
+    "setp.ne.and.u32 pp, %3, 0, pd;\n\t"                                              \
+    "setp.eq.and.u32 pq0, %3, 0, !pd;\n\t"                                            \
+    "@pp st.shared.v4.u32 [%4], {%0, %1, %2, %3};\n\t"                                \
+    "@pp mad.lo.s32 %4, %8, %11, %4;\n\t"                                             \
+    "@pd mul.lo.s32 %0, nc, %8;\n\t"                                                  \
+    "@pd mul.lo.s32 %1, xl, %8;\n\t"                                                  \
+    "@pd mul.lo.s32 %2, nr, %8;\n\t"                                                  \
+    "@pd mul.lo.s32 %3, na, %8;\n\t"                                                  \
+    "setp.ne.and.u32 pq, %4, %7, pq0;\n\t"                                            \
+    "@pq mad.lo.s32 %4, %10, %11, %4;\n\t"                                            \
+    "@pq ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n\t"                                \
+    "}\n\t"
+
 // Class registers of a lane in a DIH kernel (cls: the class index, kept for
 // the deadline dump of resumable runs).
 struct DihLane {
@@ -342,13 +398,14 @@ struct StepConsts {
 // pre-shifted left diagonal with LOP3 predicate outputs, 1 = the reference's
 // mask form with IMAD-form moves.  Kernels that count DFS nodes (NODES) step
 // every placement, so they run variant 3 when 4 is chosen; the dihedral
-// kernels run variant 1.
+// kernels run their own filtered step (NQB_STEP_DIH4) with 4, else variant 1.
 #ifndef NQB_STEP_VAR
 #define NQB_STEP_VAR 4
 #endif
 constexpr int kStepVar = NQB_STEP_VAR;
 static_assert(kStepVar == 1 || kStepVar == 3 || kStepVar == 4, "step variant");
 constexpr int kNodesStepVar = kStepVar == 4 ? 3 : kStepVar;
+constexpr int kDihStepVar = kStepVar == 4 ? 4 : 1;
 
 // Stack rows a step variant never pushes beyond the reference's N-1-rows: the
 // filtered step enters no level on row N-2 or N-1, so the deepest level it
@@ -394,14 +451,23 @@ __device__ __forceinline__ void dfs_step(uint32_t &cols, uint32_t &ld, uint32_t 
                      : "memory");
 }
 
+template <int VAR>
 __device__ __forceinline__ void dfs_step_dih(uint32_t &cols, uint32_t &ld, uint32_t &rd, uint32_t &avail, uint32_t &sp,
                                              uint32_t &cnt, uint32_t &it, uint32_t bot, const StepConsts &k,
                                              const DihLane &d, uint32_t noside) {
-    asm volatile(NQB_STEP_HEAD_DIH NQB_STEP_CHILD_DIH NQB_STEP_TAIL_VAR1
-                 : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
-                 : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(d.side_popc), "r"(d.last_mask),
-                   "r"(d.tie_bit), "r"(d.w), "r"(d.w_tie), "r"(noside)
-                 : "memory");
+    static_assert(VAR == 1 || VAR == 4, "dihedral step variants: 1 (reference form) and 4 (filtered)");
+    if constexpr (VAR == 4)
+        asm volatile(NQB_STEP_HEAD_DIH4 NQB_STEP_DIH4
+                     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
+                     : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(d.side_popc),
+                       "r"(d.last_mask), "r"(d.tie_bit), "r"(d.w), "r"(d.w_tie), "r"(noside)
+                     : "memory");
+    else
+        asm volatile(NQB_STEP_HEAD_DIH NQB_STEP_CHILD_DIH NQB_STEP_TAIL_VAR1
+                     : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt), "+r"(it)
+                     : "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(d.side_popc),
+                       "r"(d.last_mask), "r"(d.tie_bit), "r"(d.w), "r"(d.w_tie), "r"(noside)
+                     : "memory");
 }
 
 // UNROLL steps of VAR 3 (UNROLL a multiple of 4), four per asm block.
@@ -511,8 +577,11 @@ __device__ __forceinline__ uint32_t load_task(const DfsParams &p, long long t, u
 // weights, see DfsParams::cls_tab) and the step is dfs_step_dih.
 template <bool PER_OWNER, bool NODES, int VAR, int UNROLL, bool RESUME = false, bool DIH = false>
 __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
-    static_assert(!(VAR == 4 && (NODES || DIH)), "the filtered step counts no nodes and has no dihedral form");
-    static_assert(!(DIH && VAR != 1), "the dihedral step is written for the reference's mask form");
+    static_assert(!(VAR == 4 && NODES), "the filtered step counts no nodes");
+    static_assert(!DIH || VAR == 1 || VAR == 4, "dihedral step variants: 1 and 4");
+    // Lane registers and task loading of the step: the dihedral filtered step
+    // keeps VAR 3's lane form and steps rows N-2 and N-1 (no settling).
+    constexpr int LVAR = (DIH && VAR == 4) ? 3 : VAR;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long red_cnt[32];
     __shared__ unsigned long long red_nodes[32];
@@ -595,12 +664,12 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                         // a level saved by an earlier, interrupted run
                         sp = bot = my_base;
                         const uint4 e = p.cont_in[q];
-                        const int need = __popc(~e.x) - 1 - kStackRowsSpared<VAR>;
+                        const int need = __popc(~e.x) - 1 - kStackRowsSpared<LVAR>;
                         if (need > p.levels) {
                             atomicOr(p.ctl + kCtlError, kErrDepth);
                         } else {
                             cols = e.x;
-                            ld = lane_ld<VAR>(e.y);
+                            ld = lane_ld<LVAR>(e.y);
                             rd = e.z;
                             avail = e.w;
                             // a level saved on row N-2 or N-1 (by a kernel that steps those rows)
@@ -616,7 +685,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
                         // A permutation entry out of range is skipped, never dereferenced.
                         if (t >= 0 && t < p.ntasks) {
                             sp = bot = my_base;
-                            uint32_t done = load_task<VAR>(p, t, cols, ld, rd, avail);
+                            uint32_t done = load_task<LVAR>(p, t, cols, ld, rd, avail);
                             if (DIH) {
                                 load_class(p, t, dih);
                                 done *= dih.w;
@@ -693,9 +762,9 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
         if (check_idle) {
             for (int s = 0; s < p.inner; s += UNROLL) {
 #pragma unroll
-                for (int u = 0; u < (VAR >= 3 ? 1 : UNROLL); ++u) {
+                for (int u = 0; u < (VAR >= 3 && !DIH ? 1 : UNROLL); ++u) {
                     if constexpr (DIH)
-                        dfs_step_dih(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
+                        dfs_step_dih<VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
                     else if constexpr (VAR == 4)
                         dfs_steps4<UNROLL>(cols, ld, rd, avail, sp, cnt, bot, kc);
                     else if constexpr (VAR == 3)
@@ -708,9 +777,9 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
         } else {
             for (int s = 0; s < p.inner; s += UNROLL) {
 #pragma unroll
-                for (int u = 0; u < (VAR >= 3 ? 1 : UNROLL); ++u) {
+                for (int u = 0; u < (VAR >= 3 && !DIH ? 1 : UNROLL); ++u) {
                     if constexpr (DIH)
-                        dfs_step_dih(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
+                        dfs_step_dih<VAR>(cols, ld, rd, avail, sp, cnt, it, bot, kc, dih, p.noside);
                     else if constexpr (VAR == 4)
                         dfs_steps4<UNROLL>(cols, ld, rd, avail, sp, cnt, bot, kc);
                     else if constexpr (VAR == 3)
@@ -735,7 +804,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
             atomicOr(p.ctl + kCtlError, kErrContOverflow);
         } else if (mine) {
             if (avail) {
-                p.cont_out[at] = make_uint4(cols, ref_ld<VAR>(ld), rd, avail);
+                p.cont_out[at] = make_uint4(cols, ref_ld<LVAR>(ld), rd, avail);
                 if (p.cont_out_owner) p.cont_out_owner[at] = owner;
                 if (DIH) p.cont_out_cls[at] = (uint8_t)dih.cls;
                 ++at;
@@ -743,7 +812,7 @@ __global__ void __launch_bounds__(1024) dfs_kernel(DfsParams p) {
             for (uint32_t a = bot; a != sp; a += stride, ++at) {
                 uint32_t x, y, z, w;
                 lds128(a, x, y, z, w);
-                p.cont_out[at] = make_uint4(x, ref_ld<VAR>(y), z, w);
+                p.cont_out[at] = make_uint4(x, ref_ld<LVAR>(y), z, w);
                 if (p.cont_out_owner) p.cont_out_owner[at] = owner;
                 if (DIH) p.cont_out_cls[at] = (uint8_t)dih.cls;
             }
