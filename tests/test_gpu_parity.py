@@ -83,6 +83,31 @@ def test_arbitrary_32bit_inputs(gpu):
         assert np.array_equal(res["per_task"], want), N
 
 
+def test_arbitrary_inputs_on_large_boards(gpu):
+    # Boards up to N=31 with one to nine columns left, arbitrary diagonal bits
+    # (a right mask with bit 31 set shifts arithmetically, as the reference's
+    # int does) and some column masks with off-board bits: the count step's
+    # filter works on the top bit positions here (bits 29-31 of its masks).
+    rng = np.random.default_rng(29)
+    for N in (20, 24, 28, 30, 31):
+        n = 3000
+        last = (1 << N) - 1
+        cols = np.empty(n, np.uint32)
+        for i in range(n):
+            left = int(rng.integers(1, 10))
+            free = rng.choice(N, left, replace=False)
+            cols[i] = last & ~int(sum(1 << int(f) for f in free))
+        off = rng.random(n) < 0.1
+        cols[off] |= np.uint32(1 << (31 if N == 31 else N + int(rng.integers(0, 32 - N))))
+        r32 = lambda: rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+        ld = r32() & r32()
+        rd = r32() & r32()
+        rd[rng.random(n) < 0.3] |= np.uint32(0x80000000)
+        want = oracle.count_tasks(N, cols, ld, rd)
+        res = gpu.count_tasks(N, cols, ld, rd, per_task=True)
+        assert np.array_equal(res["per_task"], want), N
+
+
 def test_edge_tasks(gpu):
     N = 8
     last = (1 << N) - 1
