@@ -191,7 +191,8 @@ int nq_count_tasks(int N, const uint32_t *cols, const uint32_t *ld, const uint32
  * receives the plain sum of the counts, [1] status bits (1: a task needed
  * more stack levels than the launch had and was skipped; 2: the time limit
  * stopped the kernel).  Without a host view of the tasks the stack covers
- * N-1 levels unless cfg->stack_levels says less.  Returns after enqueueing;
+ * the deepest possible task (nq_stack_levels(N, 0, d_nodes != NULL) levels)
+ * unless cfg->stack_levels says otherwise.  Returns after enqueueing;
  * the caller synchronises the stream.  Uses the library's device scratch for the
  * queue and the per-CTA partials, so calls on one device must not overlap. */
 int nq_count_tasks_device(int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd, int64_t n,
