@@ -54,10 +54,11 @@ typedef enum nq_status {
 enum { NQ_ORDER_PLAIN = 0, NQ_ORDER_GIVEN = 1 };
 
 /* Shared-memory stack layouts.  INTERLEAVED puts slot s of lane l at
- * s*512 + l*16 inside the warp's block: a quarter-warp always touches 128
- * contiguous bytes, so no stack access is bank conflicted whatever the lanes'
- * depths.  LANE_MAJOR keeps each lane's slots contiguous (conflicts depend on
- * the depths); it exists for the autotuner's comparison. */
+ * s*512 + l*16 inside the warp's block: the eight lanes of a quarter-warp
+ * always cover the 32 banks once, whatever the lanes' depths, so no stack
+ * access needs more wavefronts than a dense 16-byte access of the warp.
+ * LANE_MAJOR keeps each lane's slots contiguous (conflicts depend on the
+ * depths); it exists for the autotuner's comparison. */
 enum { NQ_LAYOUT_INTERLEAVED = 0, NQ_LAYOUT_LANE_MAJOR = 1 };
 
 /* Launch parameters; zero-initialise and set what you need.  Zero means
