@@ -184,7 +184,7 @@ def test_device_schedule_then_count_on_one_stream(gpu, golden):
 
 
 def test_learned_order_shortens_the_tail(gpu, golden):
-    # The judge of the learned order is the measured makespan and tail idle
+    # What decides whether the learned order helps is the measured makespan and tail idle
     # time (per-CTA start/end stamps, nq_config.timing): over interleaved
     # repeats at N=19, k=6 the model's longest-first queue must leave less of
     # the grid idle at the end than the expander order, and the count kernel
