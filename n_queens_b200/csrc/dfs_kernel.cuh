@@ -241,7 +241,9 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
 // inside {b-1, b, b+1}, i.e. when no column of F0 is two or more away from
 // b.  The alive columns are therefore
 //   (columns >= lowest(F0) + 2) | (columns <= highest(F0) - 2)
-//   = -(lo << 2) | (0xffffffff >> (33 - bfind(F0)))          (empty when F0 = 0)
+//   = -(lo << 2) | (0x3fffffff >> bfind.shiftamt(F0))       (empty when F0 = 0)
+// (bfind.shiftamt is 31 - the highest set bit's position, all ones for 0, and a
+// shift by 32 or more gives 0).
 // and the child's list becomes free & that mask.  A child on row N-2 (its
 // column mask has 30 bits set, off-board bits included) is not entered: every
 // alive column of it completes the board on row N-1, so the step adds the
@@ -250,7 +252,7 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
 // 29.7e9 to 18.6e9 and the pushes from 7.8e9 to 5.0e9, for 32 instructions per
 // step instead of 20.  Tasks and saved levels on rows N-2 and N-1 are counted
 // when they are loaded.  Lane registers as in VAR 3.  Operands as in VAR 1
-// plus %12 = 33, %13 = -4, %14 = 30.
+// plus %12 = 0x3fffffff, %13 = -4, %14 = 30.
 #define NQB_STEP4_HEAD                                                                \
     "{\n\t"                                                                           \
     ".reg .pred pt1, pb, pg, p2, pd, pk, pp, pq;\n\t"                                 \
@@ -271,9 +273,8 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "mul.lo.s32 t, f0, %10;\n\t"                                                      \
     "and.b32 lo, t, f0;\n\t"                                                          \
     "mul.lo.s32 ma, lo, %13;\n\t"                                                     \
-    "bfind.u32 pos, f0;\n\t"                                                          \
-    "mad.lo.s32 pos, pos, %10, %12;\n\t"                                              \
-    "shr.b32 mb, %10, pos;\n\t"                                                       \
+    "bfind.shiftamt.u32 pos, f0;\n\t"                                                 \
+    "shr.b32 mb, %12, pos;\n\t"                                                       \
     "popc.b32 pc, nc;\n\t"                                                            \
     "setp.ne.and.u32 pg, pc, %14, pb;\n\t"                                            \
     "setp.eq.and.u32 p2, pc, %14, pb;\n\t"                                            \
@@ -500,7 +501,7 @@ __device__ __forceinline__ void dfs_steps4(uint32_t &cols, uint32_t &ld, uint32_
     for (int g = 0; g < UNROLL / 4; ++g)
         asm volatile(NQB_STEP4_HEAD NQB_STEP4_X4 "}\n\t"
                      : "+r"(cols), "+r"(ld), "+r"(rd), "+r"(avail), "+r"(sp), "+r"(cnt)
-                     : "r"(0u), "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(33u),
+                     : "r"(0u), "r"(bot), "r"(k.one), "r"(k.two), "r"(k.mone), "r"(k.stride), "r"(0x3fffffffu),
                        "r"(0xfffffffcu), "r"(30u)
                      : "memory");
 }
