@@ -252,7 +252,10 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
 // 29.7e9 to 18.6e9 and the pushes from 7.8e9 to 5.0e9, for 32 instructions per
 // step instead of 20.  Tasks and saved levels on rows N-2 and N-1 are counted
 // when they are loaded.  Lane registers as in VAR 3.  Operands as in VAR 1
-// plus %12 = 0x3fffffff, %13 = -4, %14 = 30.
+// plus %12 = 0x3fffffff, %13 = -4, %14 = 30.  Pipe balance (N=21, measured):
+// taking the highest bit's mask from bfind's shift amount instead of a
+// multiply-add saved 4.2 %, negating F0 on the ALU instead of the FMA pipe
+// 0.3 %; moving the count or the first negation to the ALU pipe did not help.
 #define NQB_STEP4_HEAD                                                                \
     "{\n\t"                                                                           \
     ".reg .pred pt1, pb, pg, p2, pd, pk, pp, pq;\n\t"                                 \
@@ -270,7 +273,7 @@ __device__ __forceinline__ void lds128(uint32_t a, uint32_t &x, uint32_t &y, uin
     "mul.lo.s32 xl, nl, %9;\n\t"                                                      \
     "shr.s32 xr, nr, 1;\n\t"                                                          \
     "lop3.b32 f0, nc, xl, xr, 0x01;\n\t"                                              \
-    "mul.lo.s32 t, f0, %10;\n\t"                                                      \
+    "neg.s32 t, f0;\n\t"                                                              \
     "and.b32 lo, t, f0;\n\t"                                                          \
     "mul.lo.s32 ma, lo, %13;\n\t"                                                     \
     "bfind.shiftamt.u32 pos, f0;\n\t"                                                 \
