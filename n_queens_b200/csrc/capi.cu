@@ -68,8 +68,8 @@ KernelFn pick_kernel(bool per_owner, bool nodes, bool dih = false) {
     if (dih) return per_owner ? dfs_kernel<true, false, kDihStepVar, kUnroll, false, true>
                               : dfs_kernel<false, false, kDihStepVar, kUnroll, false, true>;
     if (per_owner)
-        return nodes ? dfs_kernel<true, true, kNodesStepVar, kUnroll> : dfs_kernel<true, false, kStepVar, kUnroll>;
-    return nodes ? dfs_kernel<false, true, kNodesStepVar, kUnroll> : dfs_kernel<false, false, kStepVar, kUnroll>;
+        return nodes ? dfs_kernel<true, true, kNodesStepVar, kUnroll> : dfs_kernel<true, false, kStepVar, kCountUnroll>;
+    return nodes ? dfs_kernel<false, true, kNodesStepVar, kUnroll> : dfs_kernel<false, false, kStepVar, kCountUnroll>;
 }
 
 struct DevBuf {
@@ -148,7 +148,7 @@ int ensure_ready(Ctx &c, int dev) {
         for (int nd = 0; nd < 2; ++nd)
             NQ_CUDA(cudaFuncSetAttribute(pick_kernel(po, nd), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          c.smem_optin - static_smem));
-    NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, kStepVar, kUnroll, true>,
+    NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, kStepVar, kCountUnroll, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, c.smem_optin - static_smem));
     NQ_CUDA(cudaFuncSetAttribute(dfs_kernel<false, false, kDihStepVar, kUnroll, true, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, c.smem_optin - static_smem));
@@ -833,7 +833,7 @@ int count_resumable_impl(int N, int rows, const nq_config *cfg, const char *chec
         NQ_CUDA(cudaMemcpyAsync(d_cont_in, ck.cont.data(), ncont * 16, cudaMemcpyHostToDevice, c.stream));
         if (dih) NQ_CUDA(cudaMemcpyAsync(d_cont_cls, ck.cls.data(), ncont, cudaMemcpyHostToDevice, c.stream));
     }
-    KernelFn fn = dih ? dfs_kernel<false, false, kDihStepVar, kUnroll, true, true> : dfs_kernel<false, false, kStepVar, kUnroll, true>;
+    KernelFn fn = dih ? dfs_kernel<false, false, kDihStepVar, kUnroll, true, true> : dfs_kernel<false, false, kStepVar, kCountUnroll, true>;
     Launch L;
     rc = plan_launch(c, cfg, stack_need(N, rows, !dih), false, false, L, dih);
     if (rc) return rc;

@@ -62,7 +62,7 @@ NoAllocDev g_noalloc_dev[kNoAllocMaxDevices];
 
 typedef void (*NoAllocKernel)(DfsParams);
 // The same instantiation the allocating device entry runs for a plain count.
-NoAllocKernel noalloc_kernel() { return dfs_kernel<false, false, kStepVar, kUnroll>; }
+NoAllocKernel noalloc_kernel() { return dfs_kernel<false, false, kStepVar, kCountUnroll>; }
 
 int noalloc_fail(cudaError_t e, const char *what) {
     set_last_error((std::string(what) + ": " + cudaGetErrorString(e)).c_str());
