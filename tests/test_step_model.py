@@ -15,6 +15,11 @@ but changes no arithmetic), and checks three things on the CPU:
   per-task need the launch reserves for the filtered step;
 * an idle lane (no untried column, empty stack) is left unchanged by further
   steps, which is what lets a warp keep stepping while some lanes wait.
+
+The dihedral kernels' filtered step (``NQB_STEP_DIH4``: dead children dropped,
+rows N-2 and N-1 still stepped under the class rules) is restated the same way
+and checked against the oracle's weighted per-task counts of the dihedral
+decomposition (oracle/dihedral_oracle.c) and the whole-board totals.
 """
 import numpy as np
 import pytest
@@ -248,3 +253,106 @@ def test_idle_lanes_are_unchanged():
     for a, b in zip(before, (lanes.cols, lanes.ld, lanes.rd, lanes.avail, lanes.cnt, lanes.sp)):
         np.testing.assert_array_equal(a, b)
     np.testing.assert_array_equal(got, oracle_counts(N, c, l, r))
+
+
+# ---- The dihedral kernels' filtered step (NQB_STEP_DIH4) --------------------------------------------
+
+def bfind(x):
+    """bfind.u32: index of the highest set bit, 0xffffffff for 0."""
+    return np.where(x == 0, np.uint32(0xFFFFFFFF), (31 - shiftamt(x).astype(np.int64)).astype(np.uint32))
+
+
+class DihLanes:
+    """Lanes of a dihedral kernel: the task's class rules ride in per-lane registers."""
+
+    def __init__(self, N, c, l, r, cls, classes):
+        c, l, r = (np.ascontiguousarray(a, np.uint32) for a in (c, l, r))
+        cls = np.ascontiguousarray(cls, np.int64)
+        tab = np.array([(min(32 - N + s, 64), lm, tb, w, wt) for (s, lm, tb, w, wt) in classes], np.uint64)
+        self.side_popc = tab[cls, 0].astype(np.uint32)
+        self.last_mask = tab[cls, 1].astype(np.uint32)
+        self.tie_bit = tab[cls, 2].astype(np.uint32)
+        self.w = tab[cls, 3].astype(np.uint32)
+        self.w_tie = tab[cls, 4].astype(np.uint32)
+        self.noside = np.uint32(~((1 << 0) | (1 << (N - 1))) & 0xFFFFFFFF)
+        # load_task<3>: no settling; a complete board weighs the class weight.
+        last = np.uint32(0xFFFFFFFF if N >= 32 else (1 << N) - 1)
+        bad = (c & ~last) != 0
+        done = (c == last) & ~bad
+        self.cols = c | ~last
+        self.ld = l << np.uint32(1)
+        self.rd = r.copy()
+        avail = np.where(bad | done, np.uint32(0), ~(self.cols | l | r))
+        # The task's own row follows the class rules too.
+        pc = popc(self.cols)
+        rule = (avail != 0) & (pc > self.side_popc)
+        avail = np.where(rule, avail & np.where(pc == 31, self.last_mask, self.noside), avail)
+        self.avail = avail
+        self.credit = np.where(done, self.w, 0).astype(np.uint64)
+        self.n = c.size
+        self.stack = np.zeros((self.n, N + 2, 4), np.uint32)
+        self.sp = np.zeros(self.n, np.int64)
+        self.deepest = np.zeros(self.n, np.int64)
+        self.cnt = np.zeros(self.n, np.uint64)
+
+    def step(self):
+        """One NQB_STEP_DIH4 on every lane (%12 side popc, %13 row N-1 mask, %14 tie bit, %15/%16 weights,
+        %17 ~side columns)."""
+        one, two, mone, m4 = np.uint32(1), np.uint32(2), np.uint32(0xFFFFFFFF), np.uint32(0xFFFFFFFC)
+        cols, ld, rd, avail = self.cols, self.ld, self.rd, self.avail
+        t = avail * mone
+        bit = t & avail
+        pb = bit != 0
+        avail = bit * mone + avail
+        nc = bit * one + cols
+        nl = bit * two + ld
+        nr = sar1(rd | bit)
+        na = ~(nc | nl | nr)
+        pc = popc(nc)
+        ps = pc > self.side_popc
+        pl = pc == 31
+        msk = np.where(pl, self.last_mask, self.noside)
+        na = np.where(ps, na & msk, na)
+        xl = nl * two
+        xr = sar1(nr)
+        f0 = ~(nc | xl | xr)
+        t = f0 * mone
+        lo = t & f0
+        ma = lo * m4
+        pos = bfind(f0) * mone + np.uint32(33)
+        mb = shr_clamp(mone, pos)
+        na = np.where(~pl, na & (ma | mb), na)
+        pd = (na != 0) & pb
+        pe = nc == mone
+        w = np.where(bit == self.tie_bit, self.w_tie, self.w)
+        self.cnt += np.where(pe, w, 0).astype(np.uint64)
+        pp = (avail != 0) & pd
+        pq0 = (avail == 0) & ~pd
+        lanes = np.arange(self.n)
+        idx = lanes[pp]
+        self.stack[idx, self.sp[idx]] = np.stack([cols[idx], ld[idx], rd[idx], avail[idx]], axis=1)
+        self.sp[idx] += 1
+        self.deepest = np.maximum(self.deepest, self.sp)
+        cols = np.where(pd, nc, cols)
+        ld = np.where(pd, xl, ld)
+        rd = np.where(pd, nr, rd)
+        avail = np.where(pd, na, avail)
+        pq = (self.sp != 0) & pq0
+        idx = lanes[pq]
+        self.sp[idx] -= 1
+        top = self.stack[idx, self.sp[idx]]
+        cols[idx], ld[idx], rd[idx], avail[idx] = top[:, 0], top[:, 1], top[:, 2], top[:, 3]
+        self.cols, self.ld, self.rd, self.avail = cols, ld, rd, avail
+
+    run = Lanes.run
+
+
+@pytest.mark.parametrize("N,k", [(4, 2), (5, 2), (6, 2), (7, 3), (8, 3), (9, 3), (10, 4), (11, 4), (12, 5), (13, 5)])
+def test_dihedral_step_weighted_counts(N, k):
+    c, l, r, cls, classes = oracle.dihedral_expand(N, k)
+    lanes = DihLanes(N, c, l, r, cls, classes)
+    got = lanes.run()
+    np.testing.assert_array_equal(got, oracle.dihedral_count_tasks(N, k, c, l, r, cls))
+    assert int(got.sum()) == oracle.total(N, min(2, N - 2))
+    # The dihedral launch reserves N-1-popc(cols) slots (rows N-2 and N-1 are stepped).
+    assert (lanes.deepest <= np.maximum(1, N - 1 - popc(c).astype(np.int64))).all()
