@@ -36,6 +36,12 @@ extern "C" {
  * library takes any N < 32, since masks are 32-bit. */
 #define NQ_MAX_N 31
 
+/* Largest nq_config.inner_steps.  A lane's 32-bit counter is folded into its
+ * 64-bit total every inner_steps steps and a step adds at most 32, so any
+ * bound below 2^27 keeps it exact; this one is far above the useful range
+ * (256..4096). */
+#define NQ_MAX_INNER_STEPS (1 << 20)
+
 typedef enum nq_status {
     NQ_OK = 0,
     NQ_ERR_ARG = -1,       /* an argument is out of range or a pointer is NULL */
@@ -69,7 +75,9 @@ typedef struct nq_config {
     int blocks_per_sm;      /* resident CTAs per SM for the persistent grid */
     int stack_levels;       /* per-lane DFS stack slots (>= nq_stack_levels(N, rows, nodes)) */
     int steal;              /* 0 = default (on), 1 = on, -1 = off: in-warp work donation */
-    int inner_steps;        /* DFS steps between warp refill checks (multiple of 4) */
+    int inner_steps;        /* DFS steps between warp refill checks: 1..NQ_MAX_INNER_STEPS (larger values
+                               are NQ_ERR_ARG), rounded up to a multiple of the kernel's steps per warp
+                               vote (16 for counts, 8 for node counts and the dihedral kernels) */
     int order_kind;         /* NQ_ORDER_PLAIN or NQ_ORDER_GIVEN */
     const uint32_t *order;  /* NQ_ORDER_GIVEN: queue position -> task index (host or device
                                pointer, matching the entry's other task arrays) */

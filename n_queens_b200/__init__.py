@@ -42,6 +42,7 @@ NQ_ERR_NO_KERNEL = -7
 NQ_ORDER_PLAIN = 0
 NQ_ORDER_GIVEN = 1
 NQ_MAX_N = 31
+NQ_MAX_INNER_STEPS = 1 << 20
 
 
 class NQError(RuntimeError):

@@ -225,6 +225,10 @@ int plan_launch(Ctx &c, const nq_config *cfg, int levels_needed, bool per_owner,
     per_sm = std::min(per_sm, kMaxBlocksPerSm);
     if (cfg && cfg->blocks_per_sm > 0) per_sm = std::min(per_sm, cfg->blocks_per_sm);
     L.grid = c.sms * per_sm;
+    if (cfg && cfg->inner_steps > NQ_MAX_INNER_STEPS) {
+        g_last_error = "inner_steps is above NQ_MAX_INNER_STEPS";
+        return NQ_ERR_ARG;
+    }
     L.inner = (cfg && cfg->inner_steps > 0) ? ((cfg->inner_steps + 3) & ~3) : kDefaultInner;
     L.steal = (cfg && cfg->steal < 0) ? 0 : 1;
     L.layout = (cfg && cfg->layout == NQ_LAYOUT_LANE_MAJOR) ? 1 : 0;
@@ -1361,6 +1365,7 @@ int nq_batch_destroy(nq_batch *b) {
 int nq_batch_autotune(const nq_instance *inst, int64_t n, int repeats, const nq_config *base, nq_tune_entry *table,
                       int table_cap, int *n_entries, nq_tune_entry *best) {
     if (!inst || n <= 0 || repeats < 1 || !best || table_cap < 0 || (table_cap > 0 && !table)) return NQ_ERR_ARG;
+    if (base && base->inner_steps > NQ_MAX_INNER_STEPS) return NQ_ERR_ARG;
     static const int kSplits[] = {3, 4, 5, 6, 7};
     static const int kThreads[] = {64, 128, 256, 512};
     static const int kLayouts[] = {NQ_LAYOUT_INTERLEAVED, NQ_LAYOUT_LANE_MAJOR};

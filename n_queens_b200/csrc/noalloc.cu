@@ -207,6 +207,10 @@ extern "C" int nq_count_tasks_device_noalloc(int N, const uint32_t *d_cols, cons
     }
     p.N = N;
     p.levels = levels;
+    if (cfg && cfg->inner_steps > NQ_MAX_INNER_STEPS) {
+        set_last_error("inner_steps is above NQ_MAX_INNER_STEPS");
+        return NQ_ERR_ARG;
+    }
     p.inner = (cfg && cfg->inner_steps > 0) ? ((cfg->inner_steps + 3) & ~3) : kDefaultInner;
     p.steal = (cfg && cfg->steal < 0) ? 0 : 1;
     p.layout = (cfg && cfg->layout == NQ_LAYOUT_LANE_MAJOR) ? 1 : 0;

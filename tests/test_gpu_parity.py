@@ -147,6 +147,14 @@ def test_depth_error_is_reported(gpu):
     assert gpu.count(12, 4).total == 14200
 
 
+def test_inner_steps_bound(gpu):
+    with pytest.raises(gpu.NQError) as e:
+        gpu.count(12, 4, config=dict(inner_steps=gpu.NQ_MAX_INNER_STEPS + 1))
+    assert e.value.status == gpu.NQ_ERR_ARG
+    # The bound itself is accepted, and the context stays usable.
+    assert gpu.count(12, 4, config=dict(inner_steps=gpu.NQ_MAX_INNER_STEPS)).total == 14200
+
+
 def test_time_limit_stops_kernel_and_context_survives(gpu, golden):
     with pytest.raises(gpu.NQError) as e:
         gpu.count(19, 6, config=dict(time_limit_ms=1))

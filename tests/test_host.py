@@ -32,6 +32,14 @@ def test_library_exports_every_declared_symbol():
     assert nq.lib.nq_abi_version() == 1
 
 
+def test_header_constants_match_python_mirror():
+    text = open(os.path.join(ROOT, "include", "n_queens_b200.h")).read()
+    defines = dict(re.findall(r"^#define (NQ_\w+) (.+)$", text, re.M))
+    assert int(defines["NQ_MAX_N"]) == nq.NQ_MAX_N
+    assert eval(defines["NQ_MAX_INNER_STEPS"]) == nq.NQ_MAX_INNER_STEPS
+    assert int(defines["NQ_ABI_VERSION"]) == 1
+
+
 def test_dropin_cxx_symbols_exported():
     out = subprocess.run(["nm", "-D", "--defined-only", nq.LIB_PATH], capture_output=True, text=True).stdout
     for mangled in ["_Z13cuda_n_queensii", "_Z8n_queensiiiiRx"]:
