@@ -42,6 +42,11 @@ extern "C" {
  * (256..4096). */
 #define NQ_MAX_INNER_STEPS (1 << 20)
 
+/* Largest nq_config.stack_levels.  No task of a board of at most NQ_MAX_N
+ * columns needs more than N-1 <= 30 slots per lane; larger values are
+ * NQ_ERR_ARG. */
+#define NQ_MAX_STACK_LEVELS 32
+
 typedef enum nq_status {
     NQ_OK = 0,
     NQ_ERR_ARG = -1,       /* an argument is out of range or a pointer is NULL */
@@ -73,7 +78,8 @@ typedef struct nq_config {
     int block_threads;      /* threads per CTA: 32..1024, multiple of 32; 0 = the size (64..512) that keeps
                                the most warps resident per SM for the launch's stack depth */
     int blocks_per_sm;      /* resident CTAs per SM for the persistent grid */
-    int stack_levels;       /* per-lane DFS stack slots (>= nq_stack_levels(N, rows, nodes)) */
+    int stack_levels;       /* per-lane DFS stack slots (>= nq_stack_levels(N, rows, nodes), at most
+                               NQ_MAX_STACK_LEVELS) */
     int steal;              /* 0 = default (on), 1 = on, -1 = off: in-warp work donation */
     int inner_steps;        /* DFS steps between warp refill checks: 1..NQ_MAX_INNER_STEPS (larger values
                                are NQ_ERR_ARG), rounded up to a multiple of the kernel's steps per warp

@@ -43,6 +43,7 @@ NQ_ORDER_PLAIN = 0
 NQ_ORDER_GIVEN = 1
 NQ_MAX_N = 31
 NQ_MAX_INNER_STEPS = 1 << 20
+NQ_MAX_STACK_LEVELS = 32
 
 
 class NQError(RuntimeError):

@@ -190,6 +190,10 @@ int plan_launch(Ctx &c, const nq_config *cfg, int levels_needed, bool per_owner,
                 bool dih = false) {
     L.dih = dih;
     L.levels = std::max(1, levels_needed);
+    if (cfg && cfg->stack_levels > NQ_MAX_STACK_LEVELS) {
+        g_last_error = "stack_levels is above NQ_MAX_STACK_LEVELS";
+        return NQ_ERR_ARG;
+    }
     if (cfg && cfg->stack_levels > 0) {
         if (cfg->stack_levels < levels_needed) {
             g_last_error = "stack_levels is below what the tasks need";
@@ -210,11 +214,12 @@ int plan_launch(Ctx &c, const nq_config *cfg, int levels_needed, bool per_owner,
         g_last_error = "block_threads must be a multiple of 32 in [32, 1024]";
         return NQ_ERR_ARG;
     }
-    L.smem = (L.threads / 32) * L.levels * (int)kSlotBytes;
-    if (L.smem + kDfsStaticSmem > c.smem_optin) {
+    const long long smem = (long long)(L.threads / 32) * L.levels * kSlotBytes;
+    if (smem + kDfsStaticSmem > c.smem_optin) {
         g_last_error = "per-CTA stack does not fit in shared memory: lower block_threads";
         return NQ_ERR_DEPTH;
     }
+    L.smem = (int)smem;
     int per_sm = 0;
     NQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_kernel(per_owner, nodes, dih),
                                                           L.threads, L.smem));

@@ -57,10 +57,10 @@ template <typename Kernel>
 int resident_warp_threads(Kernel fn, int levels, int smem_optin, int cap_per_sm) {
     int best = 0, best_warps = 0;
     for (int t = kMaxAutoThreads; t >= kMinAutoThreads; t -= 32) {
-        const int smem = (t / 32) * levels * (int)kSlotBytes;
+        const long long smem = (long long)(t / 32) * levels * kSlotBytes;
         if (smem + kDfsStaticSmem > smem_optin) continue;
         int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, t, smem) != cudaSuccess) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, t, (size_t)smem) != cudaSuccess) {
             (void)cudaGetLastError();
             continue;
         }

@@ -166,6 +166,10 @@ extern "C" int nq_count_tasks_device_noalloc(int N, const uint32_t *d_cols, cons
     // CTA size that keeps the most warps resident for the stack depth, 1024
     // DFS steps between queue visits), with the grid bounded by the array's
     // per-CTA partials.
+    if (cfg && cfg->stack_levels > NQ_MAX_STACK_LEVELS) {
+        set_last_error("stack_levels is above NQ_MAX_STACK_LEVELS");
+        return NQ_ERR_ARG;
+    }
     const int levels = (cfg && cfg->stack_levels > 0) ? cfg->stack_levels : stack_need(N, 0, true);
     int cap_per_sm = std::min(kNoAllocMaxBlocksPerSm, std::max(1, kNoAllocMaxCtas / d.sms));
     if (cfg && cfg->blocks_per_sm > 0) cap_per_sm = std::min(cap_per_sm, cfg->blocks_per_sm);
@@ -177,11 +181,12 @@ extern "C" int nq_count_tasks_device_noalloc(int N, const uint32_t *d_cols, cons
         return NQ_ERR_DEPTH;
     }
     if (threads < 32 || threads > 1024 || (threads & 31)) return NQ_ERR_ARG;
-    const int smem = (threads / 32) * levels * (int)kSlotBytes;
-    if (smem + kDfsStaticSmem > d.smem_optin) {
+    const long long smem64 = (long long)(threads / 32) * levels * kSlotBytes;
+    if (smem64 + kDfsStaticSmem > d.smem_optin) {
         set_last_error("per-CTA stack does not fit in shared memory: lower block_threads or stack_levels");
         return NQ_ERR_DEPTH;
     }
+    const int smem = (int)smem64;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, noalloc_kernel(), threads, smem);
     if (e != cudaSuccess) return noalloc_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");

@@ -147,12 +147,15 @@ def test_depth_error_is_reported(gpu):
     assert gpu.count(12, 4).total == 14200
 
 
-def test_inner_steps_bound(gpu):
-    with pytest.raises(gpu.NQError) as e:
-        gpu.count(12, 4, config=dict(inner_steps=gpu.NQ_MAX_INNER_STEPS + 1))
-    assert e.value.status == gpu.NQ_ERR_ARG
-    # The bound itself is accepted, and the context stays usable.
+def test_config_upper_bounds(gpu):
+    for bad in (dict(inner_steps=gpu.NQ_MAX_INNER_STEPS + 1), dict(stack_levels=gpu.NQ_MAX_STACK_LEVELS + 1),
+                dict(stack_levels=1 << 18, block_threads=1024)):
+        with pytest.raises(gpu.NQError) as e:
+            gpu.count(12, 4, config=bad)
+        assert e.value.status == gpu.NQ_ERR_ARG, bad
+    # The bounds themselves are accepted, and the context stays usable.
     assert gpu.count(12, 4, config=dict(inner_steps=gpu.NQ_MAX_INNER_STEPS)).total == 14200
+    assert gpu.count(12, 4, config=dict(stack_levels=gpu.NQ_MAX_STACK_LEVELS)).total == 14200
 
 
 def test_time_limit_stops_kernel_and_context_survives(gpu, golden):

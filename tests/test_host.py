@@ -37,6 +37,10 @@ def test_header_constants_match_python_mirror():
     defines = dict(re.findall(r"^#define (NQ_\w+) (.+)$", text, re.M))
     assert int(defines["NQ_MAX_N"]) == nq.NQ_MAX_N
     assert eval(defines["NQ_MAX_INNER_STEPS"]) == nq.NQ_MAX_INNER_STEPS
+    assert int(defines["NQ_MAX_STACK_LEVELS"]) == nq.NQ_MAX_STACK_LEVELS
+    # No task of a board of at most NQ_MAX_N columns needs more slots than the bound.
+    assert max(nq.stack_levels(N, 0, nodes) for N in range(1, nq.NQ_MAX_N + 1) for nodes in (0, 1)) \
+        <= nq.NQ_MAX_STACK_LEVELS
     assert int(defines["NQ_ABI_VERSION"]) == 1
 
 
