@@ -526,6 +526,16 @@ int read_checkpoint(const char *path, int N, int rows, int mode, Checkpoint &ck,
         g_last_error = hmode ? "checkpoint is of a dihedral count" : "checkpoint is of a plain (mirror) count";
         return NQ_ERR_ARG;
     }
+    // Every continuation entry must be a level the kernel could have saved:
+    // its column mask carries the off-board columns and its untried columns
+    // are free (no column, no diagonal).  The kernel's stack bound rests on
+    // the second: a step on a column already in the mask would add no queen.
+    const uint32_t last = (N >= 32) ? 0xffffffffu : ((1u << N) - 1u);
+    for (const uint4 &e : ck.cont)
+        if ((e.x & ~last) != ~last || (e.w & (e.x | e.y | e.z)) != 0) {
+            g_last_error = "checkpoint holds a continuation entry that no count could have saved";
+            return NQ_ERR_ARG;
+        }
     ck.N = hN;
     ck.rows = hrows;
     ck.mode = hmode;

@@ -159,3 +159,34 @@ def test_resumable_checkpoint_mode_is_checked(tmp_path):
     p.write_bytes(one)                                        # an entry without its class byte
     assert nq.lib.nq_count_dihedral_resumable(10, 3, None, str(p).encode(), ctypes.byref(t), ctypes.byref(d),
                                               None) == nq.NQ_ERR_ARG
+
+
+def test_resumable_checkpoint_entries_are_checked(tmp_path):
+    # A continuation entry must carry the off-board columns and list only free columns as untried; anything
+    # else is refused before any device work (a valid file gets as far as the missing device).
+    import ctypes
+    import struct
+    p = tmp_path / "ck"
+    t = ctypes.c_uint64(0)
+    d = ctypes.c_int(0)
+    N, rows = 10, 3
+    off = 0xFFFFFFFF & ~((1 << N) - 1)
+    ntasks = nq.expand(N, rows)[0].size
+
+    def write(entries):
+        hdr = b"NQB200CK" + struct.pack("<IiiiqqQQq", 1, N, rows, 0, ntasks, 5, 7, 1, len(entries))
+        p.write_bytes(hdr + b"".join(struct.pack("<IIII", *e) for e in entries))
+
+    def run():
+        return nq.lib.nq_count_resumable(N, rows, None, str(p).encode(), ctypes.byref(t), ctypes.byref(d), None)
+
+    good = (off | 0b1, 0b10, 0, 0b1100)          # a queen in column 0; columns 2 and 3 untried
+    for bad in [(0b1, 0b10, 0, 0b1100),          # off-board columns missing
+                (off | 0b1, 0b10, 0, 0b1101),    # untried column 0 is taken
+                (off | 0b1, 0b110, 0, 0b1100),   # untried column 2 is on a left diagonal
+                (off | 0b1, 0b10, 0b1000, 0b1100)]:  # untried column 3 is on a right diagonal
+        write([good, bad])
+        assert run() == nq.NQ_ERR_ARG, bad
+        assert "continuation entry" in nq.last_error()
+    write([good])
+    assert run() in (nq.NQ_ERR_NO_DEVICE, nq.NQ_OK)
