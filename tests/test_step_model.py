@@ -356,3 +356,39 @@ def test_dihedral_step_weighted_counts(N, k):
     assert int(got.sum()) == oracle.total(N, min(2, N - 2))
     # The dihedral launch reserves N-1-popc(cols) slots (rows N-2 and N-1 are stepped).
     assert (lanes.deepest <= np.maximum(1, N - 1 - popc(c).astype(np.int64))).all()
+
+
+def saved_levels(lanes):
+    """The entries a deadline dump writes: the current level (if it has untried columns) and every stacked level,
+    with the left diagonal back in the reference's form (ld >> 1)."""
+    out = []
+    for i in range(lanes.n):
+        if lanes.avail[i]:
+            out.append((lanes.cols[i], lanes.ld[i] >> np.uint32(1), lanes.rd[i], lanes.avail[i]))
+        for s in range(lanes.sp[i]):
+            x, y, z, w = lanes.stack[i, s]
+            out.append((x, y >> np.uint32(1), z, w))
+    return np.array(out, np.uint32).reshape(-1, 4)
+
+
+@pytest.mark.parametrize("dihedral", [False, True])
+def test_saved_levels_pass_the_checkpoint_check(dihedral):
+    # The resumable entries refuse a checkpoint entry unless its column mask carries the off-board columns and
+    # its untried columns are free; every level the kernel can save mid-run passes.
+    N, k = 12, 4
+    if dihedral:
+        c, l, r, cls, classes = oracle.dihedral_expand(N, k)
+        lanes = DihLanes(N, c, l, r, cls, classes)
+    else:
+        c, l, r = oracle.expand(N, k)
+        lanes = Lanes(N, c, l, r)
+    last = np.uint32((1 << N) - 1)
+    seen = 0
+    for _ in range(6):
+        for _ in range(40):
+            lanes.step()
+        e = saved_levels(lanes)
+        seen += len(e)
+        assert ((e[:, 0] & ~last) == ~last).all()
+        assert not (e[:, 3] & (e[:, 0] | e[:, 1] | e[:, 2])).any()
+    assert seen > 1000
