@@ -268,7 +268,10 @@ typedef struct nq_tune_entry {
  * the given instances (other launch fields from `base`), then queue chunking
  * -- 256, 1024 (the default) and 4096 DFS steps between a warp's queue
  * refills -- at the fastest of those; replays each plan's graph and writes up
- * to table_cap measured entries (40 + 2), their number and the fastest. */
+ * to table_cap measured entries (40 + 2), their number and the fastest.  Each
+ * plan's stack depth is the least its subtasks need (a deeper split needs
+ * fewer slots), so the split sweep also sweeps the stack depth and the
+ * resident warps it allows; a deeper stack than that only costs occupancy. */
 int nq_batch_autotune(const nq_instance *inst, int64_t n, int repeats, const nq_config *base, nq_tune_entry *table,
                       int table_cap, int *n_entries, nq_tune_entry *best);
 
