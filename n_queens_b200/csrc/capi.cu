@@ -504,6 +504,16 @@ int read_checkpoint(const char *path, int N, int rows, int mode, Checkpoint &ck,
               std::fread(&ck.partial, 8, 1, f) == 1 && std::fread(&ck.slices, 8, 1, f) == 1 &&
               std::fread(&n_cont, 8, 1, f) == 1 && n_cont >= 0 && n_cont < (int64_t)1 << 32;
     if (ok) {
+        // The entries must fill the rest of the file exactly; checking that
+        // before sizing the buffers keeps a corrupt count from asking for
+        // gigabytes.
+        const long here = std::ftell(f);
+        ok = here >= 0 && std::fseek(f, 0, SEEK_END) == 0;
+        const long end = ok ? std::ftell(f) : -1;
+        ok = ok && end >= here && std::fseek(f, here, SEEK_SET) == 0 &&
+             (int64_t)(end - here) == n_cont * (hmode == 1 ? 17 : 16);
+    }
+    if (ok) {
         ck.cont.resize((size_t)n_cont);
         ok = n_cont == 0 || std::fread(ck.cont.data(), 16, (size_t)n_cont, f) == (size_t)n_cont;
         if (ok && hmode == 1) {

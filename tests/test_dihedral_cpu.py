@@ -190,3 +190,8 @@ def test_resumable_checkpoint_entries_are_checked(tmp_path):
         assert "continuation entry" in nq.last_error()
     write([good])
     assert run() in (nq.NQ_ERR_NO_DEVICE, nq.NQ_OK)
+    # A header that promises more entries than the file holds is refused without sizing buffers for them.
+    hdr = b"NQB200CK" + struct.pack("<IiiiqqQQq", 1, N, rows, 0, ntasks, 5, 7, 1, (1 << 32) - 1)
+    p.write_bytes(hdr + struct.pack("<IIII", *good))
+    assert run() == nq.NQ_ERR_ARG
+    assert "not a valid checkpoint" in nq.last_error()
