@@ -52,7 +52,7 @@ typedef enum nq_status {
     NQ_ERR_ARG = -1,       /* an argument is out of range or a pointer is NULL */
     NQ_ERR_NO_DEVICE = -2, /* no CUDA device (cuda_n_queens then returns -1, src/n_queens_cuda.cu:105-108) */
     NQ_ERR_CUDA = -3,      /* a CUDA runtime call failed; see nq_last_error() */
-    NQ_ERR_OOM = -4,       /* device or pinned-host allocation failed */
+    NQ_ERR_OOM = -4,       /* device, pinned-host or host allocation failed */
     NQ_ERR_DEPTH = -5,     /* a task needs more stack levels than the launch provides */
     NQ_ERR_TIMEOUT = -6,   /* the kernel reached cfg->time_limit_ms and stopped; the counts are partial */
     NQ_ERR_NO_KERNEL = -7  /* the library has no sm_100a image for this device */

@@ -21,6 +21,8 @@
 #include <chrono>
 #include <functional>
 #include <mutex>
+#include <new>
+#include <stdexcept>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -790,6 +792,23 @@ int run_batch(Ctx &c, nq_batch &B, nq_stats *st) {
 
 void set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
 
+// No exception may cross the C ABI: every exported entry ends in a
+// function-try-block whose handler returns this status for the exception in
+// flight (a host allocation that failed is NQ_ERR_OOM).
+int status_of_exception() noexcept {
+    try {
+        throw;
+    } catch (const std::bad_alloc &) {
+        g_last_error = "out of host memory";
+        return NQ_ERR_OOM;
+    } catch (const std::exception &e) {
+        g_last_error = std::string("internal error: ") + e.what();
+    } catch (...) {
+        g_last_error = "internal error";
+    }
+    return NQ_ERR_ARG;
+}
+
 }  // namespace nqb
 
 namespace nqb {
@@ -985,12 +1004,14 @@ const char *nq_status_string(int status) {
 
 const char *nq_last_error(void) { return g_last_error.c_str(); }
 
-int nq_stack_levels(int N, int rows, int nodes) {
+int nq_stack_levels(int N, int rows, int nodes) try {
     if (N < 1 || N > NQ_MAX_N || rows < 0 || rows > N) return NQ_ERR_ARG;
     return stack_need(N, rows, nodes == 0);
+} catch (...) {
+    return status_of_exception();
 }
 
-int nq_device_count(int *count) {
+int nq_device_count(int *count) try {
     if (!count) return NQ_ERR_ARG;
     int n = 0;
     cudaError_t e = cudaGetDeviceCount(&n);
@@ -1005,20 +1026,24 @@ int nq_device_count(int *count) {
     }
     *count = n;
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_expand(int N, int rows, uint32_t *cols, uint32_t *ld, uint32_t *rd, int64_t cap, int64_t *n_tasks,
-              int threads) {
+              int threads) try {
     if (N < 2 || N > NQ_MAX_N || rows < 1 || rows > N || !n_tasks || cap < 0) return NQ_ERR_ARG;
     if (cap > 0 && (!cols || !ld || !rd)) return NQ_ERR_ARG;
     const int64_t n = expand_prefixes(N, rows, cols, ld, rd, cap, threads);
     if (n < 0) return NQ_ERR_ARG;
     *n_tasks = n;
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_expand_device(int N, int rows, uint32_t *d_cols, uint32_t *d_ld, uint32_t *d_rd, int64_t cap,
-                     int64_t *n_tasks, int device, void *stream) {
+                     int64_t *n_tasks, int device, void *stream) try {
     if (N < 2 || N > NQ_MAX_N || rows < 1 || rows > N || !n_tasks || cap < 0) return NQ_ERR_ARG;
     if (cap > 0 && (!d_cols || !d_ld || !d_rd)) return NQ_ERR_ARG;
     Ctx *cp = nullptr;
@@ -1031,6 +1056,8 @@ int nq_expand_device(int N, int rows, uint32_t *d_cols, uint32_t *d_ld, uint32_t
     NQ_CUDA(expand_prefixes_device(N, rows, d_cols, d_ld, d_rd, cap, n_tasks, &c.expand_scratch.p,
                                    &c.expand_scratch.cap, (cudaStream_t)stream));
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
 
 // Expands (N, rows) into the context's task buffer on the device.
@@ -1046,7 +1073,7 @@ int device_expand_into_ctx(Ctx &c, int N, int rows, int64_t &n) {
     return n2 == n ? NQ_OK : NQ_ERR_CUDA;
 }
 
-int nq_count(int N, int rows, const nq_config *cfg, uint64_t *total, uint64_t *nodes, nq_stats *stats) {
+int nq_count(int N, int rows, const nq_config *cfg, uint64_t *total, uint64_t *nodes, nq_stats *stats) try {
     const double t0 = now_ms();
     if (stats) memset(stats, 0, sizeof(*stats));
     if (N < 2 || N > NQ_MAX_N || rows < 1 || rows > N - 2 || !total) return NQ_ERR_ARG;
@@ -1118,20 +1145,26 @@ int nq_count(int N, int rows, const nq_config *cfg, uint64_t *total, uint64_t *n
     if (nodes) *nodes = nd;
     if (stats) stats->total_ms = now_ms() - t0;
     return rc;
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_count_resumable(int N, int rows, const nq_config *cfg, const char *checkpoint_path, uint64_t *total,
-                       int *done, nq_stats *stats) {
+                       int *done, nq_stats *stats) try {
     if (stats) memset(stats, 0, sizeof(*stats));
     if (N < 2 || N > NQ_MAX_N || rows < 1 || rows > N - 2 || !total || !done || !checkpoint_path) return NQ_ERR_ARG;
     return count_resumable_impl(N, rows, cfg, checkpoint_path, false, total, done, stats);
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_count_dihedral_resumable(int N, int rows, const nq_config *cfg, const char *checkpoint_path, uint64_t *total,
-                                int *done, nq_stats *stats) {
+                                int *done, nq_stats *stats) try {
     if (stats) memset(stats, 0, sizeof(*stats));
     if (N < 4 || N > NQ_MAX_N || rows < 2 || rows > N - 2 || !total || !done || !checkpoint_path) return NQ_ERR_ARG;
     return count_resumable_impl(N, rows, cfg, checkpoint_path, true, total, done, stats);
+} catch (...) {
+    return status_of_exception();
 }
 
 }  // extern "C"
@@ -1236,18 +1269,22 @@ int count_learned_impl(int N, int rows, nq_mlp *m, const int64_t *done_idx, int6
 
 extern "C" {
 
-int nq_count_learned(int N, int rows, nq_mlp *m, const nq_config *cfg, uint64_t *total, nq_stats *stats) {
+int nq_count_learned(int N, int rows, nq_mlp *m, const nq_config *cfg, uint64_t *total, nq_stats *stats) try {
     return count_learned_impl(N, rows, m, nullptr, 0, 0, cfg, total, stats);
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_count_learned_reuse(int N, int rows, nq_mlp *m, const int64_t *done_idx, int64_t n_done, uint64_t done_sum,
-                           const nq_config *cfg, uint64_t *total, nq_stats *stats) {
+                           const nq_config *cfg, uint64_t *total, nq_stats *stats) try {
     return count_learned_impl(N, rows, m, done_idx, n_done, done_sum, cfg, total, stats);
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_count_tasks(int N, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd, int64_t n,
                    uint64_t *per_task, uint64_t *nodes_per_task, uint64_t *sum, const nq_config *cfg,
-                   nq_stats *stats) {
+                   nq_stats *stats) try {
     const double t0 = now_ms();
     if (stats) memset(stats, 0, sizeof(*stats));
     if (N < 1 || N > NQ_MAX_N || n < 0 || !sum) return NQ_ERR_ARG;
@@ -1286,11 +1323,13 @@ int nq_count_tasks(int N, const uint32_t *cols, const uint32_t *ld, const uint32
                         nullptr, stats, true);
     if (stats) stats->total_ms = now_ms() - t0;
     return rc;
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_count_tasks_device(int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd, int64_t n,
                           uint64_t *d_per_task, uint64_t *d_nodes, uint64_t *d_sum, const nq_config *cfg,
-                          void *stream) {
+                          void *stream) try {
     if (N < 1 || N > NQ_MAX_N || n < 0 || !d_sum) return NQ_ERR_ARG;
     if (n > 0 && (!d_cols || !d_ld || !d_rd)) return NQ_ERR_ARG;
     if (n > 0xffffffffll) return NQ_ERR_ARG;
@@ -1331,9 +1370,11 @@ int nq_count_tasks_device(int N, const uint32_t *d_cols, const uint32_t *d_ld, c
         }
     }
     return enqueue_dfs(c, p, L, per_owner, want_nodes, s);
+} catch (...) {
+    return status_of_exception();
 }
 
-int nq_batch_create(const nq_instance *inst, int64_t n, int split_rows, const nq_config *cfg, nq_batch **out) {
+int nq_batch_create(const nq_instance *inst, int64_t n, int split_rows, const nq_config *cfg, nq_batch **out) try {
     if (!out) return NQ_ERR_ARG;
     *out = nullptr;
     if (n < 0 || (n > 0 && !inst) || split_rows < 0 || split_rows > 8) return NQ_ERR_ARG;
@@ -1356,9 +1397,11 @@ int nq_batch_create(const nq_instance *inst, int64_t n, int split_rows, const nq
     }
     *out = b;
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
 
-int nq_batch_run(nq_batch *b, uint64_t *out, nq_stats *stats) {
+int nq_batch_run(nq_batch *b, uint64_t *out, nq_stats *stats) try {
     if (!b || (b->n_inst > 0 && !out)) return NQ_ERR_ARG;
     const double t0 = now_ms();
     if (stats) memset(stats, 0, sizeof(*stats));
@@ -1373,9 +1416,11 @@ int nq_batch_run(nq_batch *b, uint64_t *out, nq_stats *stats) {
     }
     if (stats) stats->total_ms = now_ms() - t0;
     return status_from_bits(b->h_res[2]);
+} catch (...) {
+    return status_of_exception();
 }
 
-int nq_batch_destroy(nq_batch *b) {
+int nq_batch_destroy(nq_batch *b) try {
     if (!b) return NQ_OK;
     {
         Ctx &c = g_ctx[b->device];
@@ -1385,10 +1430,12 @@ int nq_batch_destroy(nq_batch *b) {
     }
     delete b;
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_batch_autotune(const nq_instance *inst, int64_t n, int repeats, const nq_config *base, nq_tune_entry *table,
-                      int table_cap, int *n_entries, nq_tune_entry *best) {
+                      int table_cap, int *n_entries, nq_tune_entry *best) try {
     if (!inst || n <= 0 || repeats < 1 || !best || table_cap < 0 || (table_cap > 0 && !table)) return NQ_ERR_ARG;
     if (base && base->inner_steps > NQ_MAX_INNER_STEPS) return NQ_ERR_ARG;
     static const int kSplits[] = {3, 4, 5, 6, 7};
@@ -1449,10 +1496,12 @@ int nq_batch_autotune(const nq_instance *inst, int64_t n, int repeats, const nq_
     }
     if (n_entries) *n_entries = count;
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_dihedral_expand(int N, int rows, uint32_t *cols, uint32_t *ld, uint32_t *rd, uint8_t *cls, int64_t cap,
-                       int64_t *n_tasks, nq_dihedral_class *classes, int cap_classes, int *n_classes) {
+                       int64_t *n_tasks, nq_dihedral_class *classes, int cap_classes, int *n_classes) try {
     std::vector<DihClass> tab;
     if (!dihedral_classes(N, rows, tab) || cap < 0 || cap_classes < 0) return NQ_ERR_ARG;
     if (cap > 0 && (!cols || !ld || !rd || !cls)) return NQ_ERR_ARG;
@@ -1464,9 +1513,11 @@ int nq_dihedral_expand(int N, int rows, uint32_t *cols, uint32_t *ld, uint32_t *
     if (n < 0) return NQ_ERR_ARG;
     if (n_tasks) *n_tasks = n;
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
 
-int nq_count_dihedral(int N, int rows, const nq_config *cfg, uint64_t *total, nq_stats *stats) {
+int nq_count_dihedral(int N, int rows, const nq_config *cfg, uint64_t *total, nq_stats *stats) try {
     const double t0 = now_ms();
     if (stats) memset(stats, 0, sizeof(*stats));
     if (!total || N < 4 || N > NQ_MAX_N || rows < 2 || rows > N - 2) return NQ_ERR_ARG;
@@ -1505,11 +1556,13 @@ int nq_count_dihedral(int N, int rows, const nq_config *cfg, uint64_t *total, nq
     *total = sum;  // the class weights already carry every symmetry factor
     if (stats) stats->total_ms = now_ms() - t0;
     return rc;
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_count_dihedral_tasks(int N, int rows, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd,
                             const uint8_t *cls, int64_t n, uint64_t *per_task, uint64_t *sum, const nq_config *cfg,
-                            nq_stats *stats) {
+                            nq_stats *stats) try {
     const double t0 = now_ms();
     if (stats) memset(stats, 0, sizeof(*stats));
     std::vector<DihClass> tab;
@@ -1543,10 +1596,12 @@ int nq_count_dihedral_tasks(int N, int rows, const uint32_t *cols, const uint32_
                         nullptr, stats, true, nullptr, &a);
     if (stats) stats->total_ms = now_ms() - t0;
     return rc;
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_count_batch(const nq_instance *inst, int64_t n, int split_rows, uint64_t *out, const nq_config *cfg,
-                   nq_stats *stats) {
+                   nq_stats *stats) try {
     if (stats) memset(stats, 0, sizeof(*stats));
     if (n == 0) return (n < 0 || split_rows < 0 || split_rows > 8) ? NQ_ERR_ARG : NQ_OK;
     nq_batch *b = nullptr;
@@ -1555,6 +1610,8 @@ int nq_count_batch(const nq_instance *inst, int64_t n, int split_rows, uint64_t 
     rc = nq_batch_run(b, out, stats);
     nq_batch_destroy(b);
     return rc;
+} catch (...) {
+    return status_of_exception();
 }
 
 }  // extern "C"

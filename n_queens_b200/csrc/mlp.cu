@@ -38,6 +38,8 @@
 namespace nqb {
 
 void set_last_error(const char *msg);
+// Status of the exception in flight, for the entries' handlers (defined in capi.cu).
+int status_of_exception() noexcept;
 
 namespace {
 
@@ -743,7 +745,7 @@ extern "C" {
 
 int nq_mlp_num_params(void) { return kParams; }
 
-int nq_mlp_create(int device, uint64_t seed, nq_mlp **out) {
+int nq_mlp_create(int device, uint64_t seed, nq_mlp **out) try {
     if (!out) return NQ_ERR_ARG;
     *out = nullptr;
     int ndev = 0;
@@ -789,9 +791,11 @@ int nq_mlp_create(int device, uint64_t seed, nq_mlp **out) {
     p[kOffB3] = uni(1.f / std::sqrt((float)kH2));
     *out = m;
     return nq_mlp_set_params(m, p.data());
+} catch (...) {
+    return status_of_exception();
 }
 
-int nq_mlp_destroy(nq_mlp *m) {
+int nq_mlp_destroy(nq_mlp *m) try {
     if (!m) return NQ_OK;
     cudaSetDevice(m->device);
     if (m->stream) cudaStreamSynchronize(m->stream);
@@ -808,9 +812,11 @@ int nq_mlp_destroy(nq_mlp *m) {
     if (m->stream) cudaStreamDestroy(m->stream);
     delete m;
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
 
-int nq_mlp_get_params(nq_mlp *m, float *out) {
+int nq_mlp_get_params(nq_mlp *m, float *out) try {
     int rc = check_model(m);
     if (rc) return rc;
     if (!out) return NQ_ERR_ARG;
@@ -818,9 +824,11 @@ int nq_mlp_get_params(nq_mlp *m, float *out) {
     MLP_CUDA(cudaMemcpyAsync(out, m->master, kParams * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
     MLP_CUDA(cudaStreamSynchronize(m->stream));
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
 
-int nq_mlp_set_params(nq_mlp *m, const float *in) {
+int nq_mlp_set_params(nq_mlp *m, const float *in) try {
     int rc = check_model(m);
     if (rc) return rc;
     if (!in) return NQ_ERR_ARG;
@@ -833,10 +841,12 @@ int nq_mlp_set_params(nq_mlp *m, const float *in) {
     MLP_CUDA(cudaStreamSynchronize(m->stream));
     m->steps = 0;
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_mlp_predict(nq_mlp *m, int N, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd, int64_t n,
-                   float *out) {
+                   float *out) try {
     int rc = check_model(m);
     if (rc) return rc;
     if (N < 1 || N > NQ_MAX_N || n < 0 || (n > 0 && (!cols || !ld || !rd || !out))) return NQ_ERR_ARG;
@@ -853,10 +863,12 @@ int nq_mlp_predict(nq_mlp *m, int N, const uint32_t *cols, const uint32_t *ld, c
     MLP_CUDA(cudaMemcpyAsync(out, d_out, (size_t)n * 4, cudaMemcpyDeviceToHost, m->stream));
     MLP_CUDA(cudaStreamSynchronize(m->stream));
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_mlp_predict_tensor(nq_mlp *m, int N, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd, int64_t n,
-                          float *out) {
+                          float *out) try {
     int rc = check_model(m);
     if (rc) return rc;
     if (N < 1 || N > NQ_MAX_N || n < 0 || (n > 0 && (!cols || !ld || !rd || !out))) return NQ_ERR_ARG;
@@ -878,10 +890,12 @@ int nq_mlp_predict_tensor(nq_mlp *m, int N, const uint32_t *cols, const uint32_t
         return NQ_ERR_TIMEOUT;
     }
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_mlp_grad(nq_mlp *m, const uint8_t *task_n, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd,
-                const float *target, int64_t n, float *grad_out, float *loss_out) {
+                const float *target, int64_t n, float *grad_out, float *loss_out) try {
     int rc = check_model(m);
     if (rc) return rc;
     if (n <= 0 || !task_n || !cols || !ld || !rd || !target || !grad_out) return NQ_ERR_ARG;
@@ -909,11 +923,13 @@ int nq_mlp_grad(nq_mlp *m, const uint8_t *task_n, const uint32_t *cols, const ui
         *loss_out = (float)(l / (double)n);
     }
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_mlp_train(nq_mlp *m, const uint8_t *task_n, const uint32_t *cols, const uint32_t *ld, const uint32_t *rd,
                  const float *target, int64_t n, int epochs, int batch, float lr, uint64_t seed,
-                 float *epoch_loss) {
+                 float *epoch_loss) try {
     int rc = check_model(m);
     if (rc) return rc;
     if (n <= 0 || !task_n || !cols || !ld || !rd || !target || epochs < 0 || batch < kGroup || lr <= 0.f)
@@ -966,13 +982,15 @@ int nq_mlp_train(nq_mlp *m, const uint8_t *task_n, const uint32_t *cols, const u
     }
     MLP_CUDA(cudaStreamSynchronize(m->stream));
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
 
 // Longest-first order of device-resident tasks: predictions -> keys in
 // 1/8-log2 bins -> stable descending radix sort of task indices.
 int nq_schedule_device_last(nq_mlp *m, int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd,
                             int64_t n, const uint32_t *d_last, int64_t n_last, uint32_t *d_order, float *d_pred,
-                            void *stream) {
+                            void *stream) try {
     int rc = check_model(m);
     if (rc) return rc;
     if (N < 1 || N > NQ_MAX_N || n < 0 || n > 0xffffffffll || (n > 0 && (!d_cols || !d_ld || !d_rd || !d_order)))
@@ -1004,11 +1022,15 @@ int nq_schedule_device_last(nq_mlp *m, int N, const uint32_t *d_cols, const uint
     if (rc) return rc;
     MLP_CUDA(cub::DeviceRadixSort::SortPairsDescending(m->sort_tmp, tmp, key, key2, idx, d_order, (int)n, 0, 16, s));
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
 
 int nq_schedule_device(nq_mlp *m, int N, const uint32_t *d_cols, const uint32_t *d_ld, const uint32_t *d_rd,
-                       int64_t n, uint32_t *d_order, float *d_pred, void *stream) {
+                       int64_t n, uint32_t *d_order, float *d_pred, void *stream) try {
     return nq_schedule_device_last(m, N, d_cols, d_ld, d_rd, n, nullptr, 0, d_order, d_pred, stream);
+} catch (...) {
+    return status_of_exception();
 }
 
 }  // extern "C"

@@ -37,6 +37,8 @@ namespace nqb {
 
 // Sets the text returned by nq_last_error() (defined in capi.cu).
 void set_last_error(const char *msg);
+// Status of the exception in flight, for the entry's handler (defined in capi.cu).
+int status_of_exception() noexcept;
 
 namespace {
 
@@ -132,7 +134,7 @@ using namespace nqb;
 
 extern "C" int nq_count_tasks_device_noalloc(int N, const uint32_t *d_cols, const uint32_t *d_ld,
                                              const uint32_t *d_rd, int64_t n, uint64_t *d_sum,
-                                             const nq_config *cfg, void *stream) {
+                                             const nq_config *cfg, void *stream) try {
     if (N < 1 || N > NQ_MAX_N || n < 0 || n > 0xffffffffll || !d_sum) return NQ_ERR_ARG;
     if (n > 0 && (!d_cols || !d_ld || !d_rd)) return NQ_ERR_ARG;
     const int dev = cfg ? cfg->device : 0;
@@ -240,4 +242,6 @@ extern "C" int nq_count_tasks_device_noalloc(int N, const uint32_t *d_cols, cons
     e = cudaGetLastError();
     if (e != cudaSuccess) return noalloc_fail(e, "dfs_kernel launch");
     return NQ_OK;
+} catch (...) {
+    return status_of_exception();
 }
