@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import n_queens_b200 as nq
+import oracle
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -58,6 +59,17 @@ def test_host_expander_matches_reference_bytes(golden):
             aos = np.stack([c, l, r], axis=1).view(np.int32)
             assert aos.shape[0] == case["tasks"]
             assert sha(aos) == case["sha256_aos_int32"], (case["N"], case["k"], threads)
+
+
+def test_host_expander_equals_oracle_for_every_small_case():
+    # Every (N, k) up to N=20, k=6 and three thread counts: the parallel expander keeps the reference's order.
+    for N in range(2, 21):
+        for k in range(1, min(N, 6) + 1):
+            want = oracle.expand(N, k)
+            for threads in (1, 3, 0):
+                got = nq.expand(N, k, threads=threads)
+                for g, w in zip(got, want):
+                    assert np.array_equal(g, w), (N, k, threads)
 
 
 def test_host_expander_task_counts_match_logs(golden):
